@@ -1,0 +1,194 @@
+/*
+ * lsb — a B200-native (sm_100a) slab-list hash map (uint64 -> uint64) and
+ * set (uint32) with the batched API of depaulmillz/lslab.
+ *
+ * Plain C ABI: opaque handles, device pointers, sizes, a CUDA stream.  Every
+ * batched call is asynchronous and stream-ordered, like the reference's
+ * <<<...>>> launches, and returns an int status for what can be checked on
+ * the host (LSB_ERR_ARG, launch failures).  Errors raised on the device
+ * (slab pool exhausted, a bounded wait that gave up) are recorded in the
+ * table's status word and read with lsb_map_status / lsb_set_status.  The
+ * reference has no error return at all: it exits or traps
+ * (include/lslab/lslab.h:28-41, include/lslab/detail/device_allocator.h:65-68).
+ *
+ * Batch semantics (all entry points): the ops of one call take effect as if
+ * run one at a time in index order.  The reference gives that order within
+ * each warp (lane order, include/lslab/detail/traverse.h:45-48) and an
+ * unspecified order across warps; this library gives it across the whole
+ * call, so results are deterministic, equal to a sequential replay, and for
+ * batches without same-key conflicts equal to the reference's.
+ *
+ * Concurrency: calls on one table must be ordered on one stream when any of
+ * them mutates.  Concurrent read-only calls are fine.
+ */
+#ifndef LSB_H
+#define LSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define LSB_OK 0
+#define LSB_ERR_ARG 1     /* bad handle, null pointer, size over a limit   */
+#define LSB_ERR_OOM 2     /* slab pool or device memory exhausted          */
+#define LSB_ERR_TIMEOUT 3 /* a bounded device wait gave up (lock, barrier) */
+#define LSB_ERR_CUDA 4    /* a CUDA runtime call failed                    */
+#define LSB_ERR_STATE 5   /* call not valid in the object's current state  */
+
+/* Device status bits (lsb_map_status / lsb_set_status). */
+#define LSB_STATUS_OOM 0x1u
+#define LSB_STATUS_TIMEOUT 0x2u
+#define LSB_STATUS_CHAIN 0x4u   /* a chain walk hit its hop limit */
+#define LSB_STATUS_BARRIER 0x8u /* a grid barrier gave up          */
+
+/* ---- op codes of mixed batches -------------------------------------- */
+#define LSB_OP_GET 0u
+#define LSB_OP_PUT 1u
+#define LSB_OP_REMOVE 2u
+#define LSB_OP_CONTAINS 0u /* set */
+#define LSB_OP_INSERT 1u   /* set */
+
+/* Result of a map get/remove (and of every op of a mixed batch).  Layout of
+ * cuda::std::pair<bool, uint64_t> as written by the reference's get kernel
+ * (include/lslab/detail/map_kernels.h:53-70): bool at byte 0, value at 8.
+ * On a miss the value is 0 (the reference leaves it unwritten).  For a put in
+ * a mixed batch: found = the key existed, value = the old value or 0. */
+typedef struct lsb_result {
+  uint8_t found;
+  uint8_t pad[7];
+  uint64_t value;
+} lsb_result;
+
+/* Layout of cuda::std::pair<uint64_t, uint64_t> (AoS put input,
+ * include/lslab/map.h:189-192). */
+typedef struct lsb_kv {
+  uint64_t key;
+  uint64_t value;
+} lsb_kv;
+
+typedef struct lsb_map lsb_map;
+typedef struct lsb_set lsb_set;
+
+/* Creation options; zero-initialise and set what you need. */
+typedef struct lsb_options {
+  uint64_t pool_slabs;   /* overflow slab pool; 0 = default (see lsb_map_create) */
+  uint32_t max_window;   /* ops per internal window (scratch size); 0 = 2^20     */
+  uint32_t lock_mode;    /* LSB_LOCK_*; 0 = LSB_LOCK_WRITER                     */
+  int device;            /* CUDA device; -1 = current                            */
+} lsb_options;
+
+#define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */
+#define LSB_LOCK_FREE 1u     /* writers claim slots with CAS on slab words, no lock   */
+#define LSB_LOCK_RW 2u       /* reference-style: readers take a shared bucket lock too */
+
+/* ---- map<uint64_t, uint64_t> ------------------------------------------
+ * Replaces lslab::map<K,V>::map(unsigned n_log_2) (include/lslab/map.h:43-52)
+ * and map(n_log_2, Allocator&&) (include/lslab/map.h:57-66): 2^log2_buckets
+ * head slabs plus an overflow pool of pool_slabs slabs (the reference's
+ * device_allocator(stack_size), include/lslab/device_allocator.h:16;
+ * default when 0: 2^log2_buckets / 4 + 4096). */
+int lsb_map_create(unsigned log2_buckets, uint64_t pool_slabs, lsb_map** out);
+int lsb_map_create_ex(unsigned log2_buckets, const lsb_options* opt, lsb_map** out);
+int lsb_map_destroy(lsb_map* m);
+
+/* lslab::map::get<bs>(K*, pair<bool,V>*, size_t, cudaStream_t),
+ * include/lslab/map.h:208-211 -> map_kernels::get_, map_kernels.h:53-70. */
+int lsb_map_get(lsb_map* m, const uint64_t* keys, lsb_result* out, size_t n,
+                cudaStream_t stream);
+
+/* lslab::map::put<bs>(K*, V*, V* old, size_t, cudaStream_t),
+ * include/lslab/map.h:198-201 -> map_kernels::put_ (SoA), map_kernels.h:32-50.
+ * old_out[i] = value before put i (0 if the key was absent); may be NULL. */
+int lsb_map_put(lsb_map* m, const uint64_t* keys, const uint64_t* vals, uint64_t* old_out,
+                size_t n, cudaStream_t stream);
+
+/* lslab::map::put<bs>(pair<K,V>*, V*, size_t, cudaStream_t),
+ * include/lslab/map.h:189-192 -> map_kernels::put_ (AoS), map_kernels.h:12-30. */
+int lsb_map_put_pairs(lsb_map* m, const lsb_kv* ops, uint64_t* old_out, size_t n,
+                      cudaStream_t stream);
+
+/* Map remove: the REMOVE branch of detail::traverse
+ * (include/lslab/detail/traverse.h:88-91), which the reference map does not
+ * expose.  out[i] = {found, old value or 0}; out may be NULL. */
+int lsb_map_remove(lsb_map* m, const uint64_t* keys, lsb_result* out, size_t n,
+                   cudaStream_t stream);
+
+/* Mixed batch (types[i] in LSB_OP_GET/PUT/REMOVE), run as internal windows of
+ * per-phase launches.  vals is read for puts only and may be NULL when the
+ * batch has none.  out[i] as described at lsb_result; may be NULL. */
+int lsb_map_execute(lsb_map* m, const uint8_t* types, const uint64_t* keys,
+                    const uint64_t* vals, lsb_result* out, size_t n, cudaStream_t stream);
+
+/* The same batch through one persistent cooperative launch (every phase of
+ * every window inside one kernel, grid-wide barriers between phases). */
+int lsb_map_execute_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys,
+                          const uint64_t* vals, lsb_result* out, size_t n,
+                          cudaStream_t stream);
+
+/* lslab::map::buckets(), include/lslab/map.h:225-227. */
+uint32_t lsb_map_buckets(const lsb_map* m);
+
+/* Device status bits seen since the last call (synchronises the stream),
+ * then clears them. */
+int lsb_map_status(lsb_map* m, uint32_t* flags, cudaStream_t stream);
+
+/* Slabs handed out from the overflow pool so far, and its capacity
+ * (synchronises the stream). */
+int lsb_map_pool_usage(lsb_map* m, uint64_t* used, uint64_t* capacity, cudaStream_t stream);
+
+/* Number of live entries (synchronises the stream). */
+int lsb_map_size(lsb_map* m, uint64_t* count, cudaStream_t stream);
+
+/* Copy every live (key, value) pair to HOST arrays, in key order.  *count
+ * receives the number of live entries; at most cap pairs are written.
+ * Synchronises the stream. */
+int lsb_map_dump(lsb_map* m, uint64_t* keys_out, uint64_t* vals_out, size_t cap,
+                 uint64_t* count, cudaStream_t stream);
+
+/* ---- set<uint32_t> ---------------------------------------------------
+ * Replaces lslab::set<K>::set(n_log_2[, Allocator&&]), include/lslab/set.h:267-287. */
+int lsb_set_create(unsigned log2_buckets, uint64_t pool_slabs, lsb_set** out);
+int lsb_set_create_ex(unsigned log2_buckets, const lsb_options* opt, lsb_set** out);
+int lsb_set_destroy(lsb_set* s);
+
+/* lslab::set::insert<bs>(const K*, bool*, size_t, cudaStream_t),
+ * include/lslab/set.h:339-342 -> set_kernels::insert_, set_kernels.h:47-63.
+ * Like the reference, out[i] is true for a new AND for an existing key
+ * (include/lslab/detail/traverse.h:204-212,226-232). */
+int lsb_set_insert(lsb_set* s, const uint32_t* keys, bool* out, size_t n, cudaStream_t stream);
+
+/* lslab::set::contains<bs>, include/lslab/set.h:328-331 -> set_kernels.h:28-44. */
+int lsb_set_contains(lsb_set* s, const uint32_t* keys, bool* out, size_t n,
+                     cudaStream_t stream);
+
+/* lslab::set::remove<bs>, include/lslab/set.h:350-353 -> set_kernels.h:10-26.
+ * out[i] = the key was present. */
+int lsb_set_remove(lsb_set* s, const uint32_t* keys, bool* out, size_t n, cudaStream_t stream);
+
+/* Mixed set batch (types[i] in LSB_OP_CONTAINS/INSERT/REMOVE). */
+int lsb_set_execute(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool* out,
+                    size_t n, cudaStream_t stream);
+int lsb_set_execute_fused(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool* out,
+                          size_t n, cudaStream_t stream);
+
+uint32_t lsb_set_buckets(const lsb_set* s); /* lslab::set::buckets(), set.h:361-363 */
+int lsb_set_status(lsb_set* s, uint32_t* flags, cudaStream_t stream);
+int lsb_set_pool_usage(lsb_set* s, uint64_t* used, uint64_t* capacity, cudaStream_t stream);
+int lsb_set_size(lsb_set* s, uint64_t* count, cudaStream_t stream);
+int lsb_set_dump(lsb_set* s, uint32_t* keys_out, size_t cap, uint64_t* count,
+                 cudaStream_t stream);
+
+/* ---- misc ------------------------------------------------------------- */
+const char* lsb_error_string(int code);
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int lsb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSB_H */

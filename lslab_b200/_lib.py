@@ -1,0 +1,127 @@
+"""ctypes binding of liblsb.so (the C-ABI declared in include/lsb.h).
+
+Loading fails loudly: there is no CPU fallback anywhere in the package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+from .build import LIB, ROOT
+
+HEADER = ROOT / "include" / "lsb.h"
+
+LSB_OK = 0
+LSB_ERR_ARG = 1
+LSB_ERR_OOM = 2
+LSB_ERR_TIMEOUT = 3
+LSB_ERR_CUDA = 4
+LSB_ERR_STATE = 5
+
+STATUS_OOM = 0x1
+STATUS_TIMEOUT = 0x2
+STATUS_CHAIN = 0x4
+STATUS_BARRIER = 0x8
+
+OP_GET = 0
+OP_PUT = 1
+OP_REMOVE = 2
+OP_CONTAINS = 0
+OP_INSERT = 1
+
+LOCK_WRITER = 0
+LOCK_FREE = 1
+LOCK_RW = 2
+
+
+class LsbError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {error_string(code)} (code {code})")
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("pool_slabs", C.c_uint64),
+        ("max_window", C.c_uint32),
+        ("lock_mode", C.c_uint32),
+        ("device", C.c_int),
+    ]
+
+
+_lib: C.CDLL | None = None
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+_U64 = C.c_uint64
+_U32 = C.c_uint32
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "lsb_map_create": (C.c_int, [C.c_uint, _U64, C.POINTER(_P)]),
+    "lsb_map_create_ex": (C.c_int, [C.c_uint, C.POINTER(Options), C.POINTER(_P)]),
+    "lsb_map_destroy": (C.c_int, [_P]),
+    "lsb_map_get": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_put": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
+    "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_execute": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
+    "lsb_map_execute_fused": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
+    "lsb_map_buckets": (_U32, [_P]),
+    "lsb_map_status": (C.c_int, [_P, C.POINTER(_U32), _P]),
+    "lsb_map_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
+    "lsb_map_size": (C.c_int, [_P, C.POINTER(_U64), _P]),
+    "lsb_map_dump": (C.c_int, [_P, _P, _P, _SZ, C.POINTER(_U64), _P]),
+    "lsb_set_create": (C.c_int, [C.c_uint, _U64, C.POINTER(_P)]),
+    "lsb_set_create_ex": (C.c_int, [C.c_uint, C.POINTER(Options), C.POINTER(_P)]),
+    "lsb_set_destroy": (C.c_int, [_P]),
+    "lsb_set_insert": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_set_contains": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_set_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_set_execute": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
+    "lsb_set_execute_fused": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
+    "lsb_set_buckets": (_U32, [_P]),
+    "lsb_set_status": (C.c_int, [_P, C.POINTER(_U32), _P]),
+    "lsb_set_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
+    "lsb_set_size": (C.c_int, [_P, C.POINTER(_U64), _P]),
+    "lsb_set_dump": (C.c_int, [_P, _P, _SZ, C.POINTER(_U64), _P]),
+    "lsb_error_string": (C.c_char_p, [C.c_int]),
+    "lsb_version": (C.c_int, []),
+}
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/lsb.h."""
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lsb_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> C.CDLL:
+    """Load liblsb.so (built in-tree); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            raise RuntimeError(
+                f"{LIB} is missing: build it with `python -m lslab_b200.build` "
+                "(the package has no CPU fallback)")
+        h = C.CDLL(str(LIB))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+def error_string(code: int) -> str:
+    try:
+        return lib().lsb_error_string(code).decode()
+    except Exception:  # the library itself failed to load
+        return f"error {code}"
+
+
+def check(code: int, what: str) -> None:
+    if code != LSB_OK:
+        raise LsbError(code, what)

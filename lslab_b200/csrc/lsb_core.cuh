@@ -1,0 +1,556 @@
+// Device building blocks of the slab-list table: layout, hashing, the
+// thread-per-op probe, the single-writer apply, the slab pool and the bounded
+// grid barrier.  sm_100a only.
+//
+// Layout (one slab, both containers)
+//   bytes 0..31   meta sector: u32 next (slab index, 0 = none), 28 tag bytes
+//   bytes 32..    28 slots: map = {u64 key, u64 value} (16 B), set = u32 key
+//   map slab 480 B (15 sectors), set slab 160 B (5 sectors, 16 B spare)
+// Slab indices [0, 2^n) are the bucket heads, [2^n, 2^n + pool) the overflow
+// pool, so index 0 (a head) never appears as a link and means "none".
+//
+// Tag byte: 0x00 empty (never used), 0x80 busy (being claimed), 0x80|fp live,
+// fp dead (removed; key kept so a later insert of the same key revives it).
+// fp in 1..127 comes from the high half of the hash; the bucket from the low.
+//
+// Reference counterparts: slab_node/set_node (include/lslab/detail/slab_node.h:13-35:
+// 31 keys + valid bitmap + next in lane 31's slot, values in a second array),
+// traverse (include/lslab/detail/traverse.h:27-264), warp_mutex
+// (include/lslab/warp_mutex.h:13-138), device_allocator
+// (include/lslab/detail/device_allocator.h:63-73), hash (include/lslab/hash.h:10-15).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lsb {
+
+constexpr int kSlots = 28;
+constexpr uint32_t kMetaBytes = 32;
+
+enum : uint32_t {
+  kStatusOOM = 0x1u,
+  kStatusTimeout = 0x2u,
+  kStatusChain = 0x4u,
+  kStatusBarrier = 0x8u,
+};
+
+enum : uint8_t { kOpRead = 0, kOpWrite = 1, kOpRemove = 2 };  // get/contains, put/insert, remove
+
+enum : uint32_t { kLockWriter = 0, kLockFree = 1, kLockRW = 2 };
+
+// Bounded waits: a lock or barrier wait gives up after this many polls and
+// raises kStatusTimeout / kStatusBarrier instead of spinning forever.
+constexpr uint32_t kLockPolls = 1u << 22;
+constexpr uint32_t kBarrierPolls = 1u << 24;
+constexpr uint32_t kMaxHops = 1u << 22;
+
+// ------------------------------------------------------------------ hashing
+// MurmurHash3's 64-bit finaliser (Appleby, public domain): a bijection on
+// u64, so distinct keys never collide before the bucket mask.  Replaces the
+// reference's identity hash (include/lslab/hash.h:12-14), which maps
+// sequential keys to sequential buckets and structured keys to few buckets.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+__device__ __forceinline__ uint32_t fingerprint(uint64_t h) {
+  return 1u + (uint32_t)(((h >> 32) * 127ull) >> 32);  // 1..127
+}
+
+// ------------------------------------------------------------- memory ops
+// Table reads go to L2 (.cg / .relaxed.gpu): the persistent kernel reads
+// slabs that other SMs wrote earlier in the same launch, and L1 is not
+// coherent across SMs.
+__device__ __forceinline__ uint4 ld_cg_v4(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ ulonglong2 ld_cg_v2u64(const void* p) {
+  ulonglong2 r;
+  asm volatile("ld.global.cg.v2.u64 {%0,%1}, [%2];" : "=l"(r.x), "=l"(r.y) : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t ld_cg_u32(const void* p) {
+  uint32_t r;
+  asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(r) : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ uint64_t ld_cg_u64(const void* p) {
+  uint64_t r;
+  asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(r) : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t r;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
+  return r;
+}
+
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+  uint64_t r;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(r) : "l"(p) : "memory");
+  return r;
+}
+
+__device__ __forceinline__ void st_cg_u8(void* p, uint8_t v) {
+  asm volatile("st.global.cg.u8 [%0], %1;" ::"l"(p), "h"((unsigned short)v) : "memory");
+}
+
+__device__ __forceinline__ void st_cg_u32(void* p, uint32_t v) {
+  asm volatile("st.global.cg.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_cg_u64(void* p, uint64_t v) {
+  asm volatile("st.global.cg.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_cg_v2u64(void* p, uint64_t a, uint64_t b) {
+  asm volatile("st.global.cg.v2.u64 [%0], {%1,%2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
+__device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bits) {
+  atomicOr(status, bits);
+}
+
+// ---------------------------------------------------------------- meta
+struct Meta {
+  uint32_t next;
+  uint32_t tag[7];  // 28 tag bytes, slot s in byte (s & 3) of word s >> 2
+};
+
+__device__ __forceinline__ Meta load_meta(const uint8_t* slab) {
+  uint4 a = ld_cg_v4(slab);
+  uint4 b = ld_cg_v4(slab + 16);
+  Meta m;
+  m.next = a.x;
+  m.tag[0] = a.y; m.tag[1] = a.z; m.tag[2] = a.w;
+  m.tag[3] = b.x; m.tag[4] = b.y; m.tag[5] = b.z; m.tag[6] = b.w;
+  return m;
+}
+
+// Bit s set iff tag byte s equals the byte replicated in rep4.
+__device__ __forceinline__ uint32_t tag_match(const Meta& m, uint32_t rep4) {
+  uint32_t mask = 0;
+#pragma unroll
+  for (int w = 0; w < 7; ++w) {
+    uint32_t eq = __vcmpeq4(m.tag[w], rep4);  // 0xFF per equal byte
+    // gather one bit per byte: byte j -> bit j
+    uint32_t b = (eq >> 7) & 0x01010101u;     // bits 0, 8, 16, 24
+    b = b | (b >> 7);                          // + bits 1 (byte 1), 17 (byte 3)
+    b = (b | (b >> 14)) & 0xFu;                // bits 16, 17 -> 2, 3
+    mask |= b << (4 * w);
+  }
+  return mask;
+}
+
+__device__ __forceinline__ uint8_t* slab_ptr(uint8_t* base, uint32_t idx, uint32_t bytes) {
+  return base + (size_t)idx * bytes;
+}
+__device__ __forceinline__ const uint8_t* slab_ptr(const uint8_t* base, uint32_t idx,
+                                                   uint32_t bytes) {
+  return base + (size_t)idx * bytes;
+}
+
+// -------------------------------------------------------------- traits
+struct MapTraits {
+  using Key = uint64_t;
+  static constexpr uint32_t kSlabBytes = 480;
+  static constexpr uint32_t kSlotBytes = 16;
+  static constexpr bool kHasValue = true;
+  // A dead slot may be reused only by its own key: a lock-free reader that
+  // matched the old key could otherwise read the new key's value.
+  static constexpr bool kReuseDead = false;
+  __device__ static uint64_t hash(Key k) { return mix64(k); }
+};
+
+struct SetTraits {
+  using Key = uint32_t;
+  static constexpr uint32_t kSlabBytes = 160;
+  static constexpr uint32_t kSlotBytes = 4;
+  static constexpr bool kHasValue = false;
+  // Without values a reader only ever compares the key itself, so any dead
+  // slot can take a new key.
+  static constexpr bool kReuseDead = true;
+  __device__ static uint64_t hash(Key k) { return mix64((uint64_t)k); }
+};
+
+// Device view of one table; passed by value to kernels.
+struct TableView {
+  uint8_t* slabs;      // (buckets + pool) slabs
+  int32_t* locks;      // one per bucket (reference encoding: 0 free, -1 writer, >0 readers)
+  uint32_t* status;    // device status bits
+  uint64_t* pool;      // [0] global cursor, [1] limit, [2 .. 2+kPoolSlots) per-SM ranges
+  uint32_t mask;       // buckets - 1
+  uint32_t lock_mode;
+  uint32_t chunk;      // slabs per per-SM refill (smaller for small pools)
+};
+
+constexpr int kPoolSlots = 256;
+constexpr uint32_t kPoolChunkMax = 32;
+
+// ------------------------------------------------------------ slab pool
+// Per-SM bump ranges refilled in chunks from one global cursor.  A range is
+// one u64 {end:32 | cur:32}; atomicAdd on it hands out cur.  When a range is
+// spent the thread takes a fresh chunk from the global cursor and installs
+// it; if two threads refill the same SM at once the later install wins and
+// the rest of the earlier chunk is never handed out (at most chunk - 1 slabs
+// per race).  The chunk shrinks with the pool (down to 1 slab, i.e. a plain
+// global bump) so that per-SM ranges cannot strand a small pool.  Pool memory is zeroed at creation and slabs are never
+// returned, so a slab is always empty when handed out.  Replaces the
+// reference's single global fetch_add with __trap on overflow
+// (include/lslab/detail/device_allocator.h:63-70): here exhaustion returns 0
+// and raises kStatusOOM.
+__device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
+  uint32_t smid;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  unsigned long long* range = (unsigned long long*)&t.pool[2 + (smid & (kPoolSlots - 1))];
+  unsigned long long old = atomicAdd(range, 1ull);
+  uint32_t cur = (uint32_t)old, end = (uint32_t)(old >> 32);
+  if (cur < end) return cur;
+  unsigned long long base = atomicAdd((unsigned long long*)&t.pool[0], (unsigned long long)t.chunk);
+  unsigned long long limit = t.pool[1];
+  if (base >= limit) {
+    raise_status(t.status, kStatusOOM);
+    return 0;
+  }
+  unsigned long long stop = base + t.chunk;
+  if (stop > limit) stop = limit;
+  if (base + 1 < stop) atomicExch(range, (stop << 32) | (base + 1));
+  return (uint32_t)base;
+}
+
+// --------------------------------------------------------------- locks
+__device__ __forceinline__ bool lock_writer(const TableView& t, uint32_t bucket) {
+  int32_t* l = &t.locks[bucket];
+  for (uint32_t it = 0; it < kLockPolls; ++it) {
+    if (atomicCAS(l, 0, -1) == 0) {
+      __threadfence();
+      return true;
+    }
+    __nanosleep(it < 16 ? 32 : 256);
+  }
+  raise_status(t.status, kStatusTimeout);
+  return false;
+}
+
+__device__ __forceinline__ void unlock_writer(const TableView& t, uint32_t bucket) {
+  __threadfence();
+  atomicExch(&t.locks[bucket], 0);
+}
+
+// Reference-style shared lock (include/lslab/warp_mutex.h:33-53), taken per
+// op only in LSB_LOCK_RW mode, for the locking comparison.
+__device__ __forceinline__ bool lock_reader(const TableView& t, uint32_t bucket) {
+  int32_t* l = &t.locks[bucket];
+  for (uint32_t it = 0; it < kLockPolls; ++it) {
+    int32_t p = *(volatile int32_t*)l;
+    if (p >= 0 && atomicCAS(l, p, p + 1) == p) {
+      __threadfence();
+      return true;
+    }
+  }
+  raise_status(t.status, kStatusTimeout);
+  return false;
+}
+
+__device__ __forceinline__ void unlock_reader(const TableView& t, uint32_t bucket) {
+  __threadfence();
+  atomicSub(&t.locks[bucket], 1);
+}
+
+// ---------------------------------------------------------------- probe
+// Thread-per-op lookup: per slab one 32-B meta sector, then one slot load per
+// fingerprint candidate.  Returns 1 if found (value in *val for the map).
+template <class Tr>
+__device__ __forceinline__ bool table_find(const TableView& t, typename Tr::Key key, uint64_t h,
+                                           uint64_t* val) {
+  uint32_t s = (uint32_t)h & t.mask;
+  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
+  for (uint32_t hop = 0; hop < kMaxHops; ++hop) {
+    const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
+    Meta m = load_meta(slab);
+    uint32_t cand = tag_match(m, rep);
+    while (cand) {
+      int slot = __ffs(cand) - 1;
+      cand &= cand - 1;
+      if constexpr (Tr::kHasValue) {
+        ulonglong2 kv = ld_cg_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
+        if (kv.x == (uint64_t)key) {
+          *val = kv.y;
+          return true;
+        }
+      } else {
+        uint32_t k = ld_cg_u32(slab + kMetaBytes + slot * Tr::kSlotBytes);
+        if (k == (uint32_t)key) return true;
+      }
+    }
+    s = m.next;
+    if (s == 0) return false;
+  }
+  raise_status(t.status, kStatusChain);
+  return false;
+}
+
+// ---------------------------------------------------------------- apply
+// Make the table hold `key` (present) with `val`, or not hold it (!present).
+// Exactly one thread applies a given key at a time (the batch engine groups
+// same-key ops and lets only the group's last op write), so a key's slot is
+// only ever written by that thread.  Different keys of one bucket are kept
+// apart by the bucket lock (kLockWriter / kLockRW) or by CAS on the tag and
+// link words (kLockFree).  Order of writes for an insert: slot contents,
+// fence, tag byte (or link word): a lock-free reader that sees the live tag
+// sees the slot.
+template <class Tr>
+__device__ __forceinline__ void key_store(uint8_t* slot_ptr, typename Tr::Key key, uint64_t val) {
+  if constexpr (Tr::kHasValue)
+    st_cg_v2u64(slot_ptr, (uint64_t)key, val);
+  else
+    st_cg_u32(slot_ptr, (uint32_t)key);
+}
+
+template <class Tr>
+__device__ __forceinline__ typename Tr::Key key_load(const uint8_t* slot_ptr) {
+  if constexpr (Tr::kHasValue)
+    return (typename Tr::Key)ld_cg_u64(slot_ptr);
+  else
+    return (typename Tr::Key)ld_cg_u32(slot_ptr);
+}
+
+struct ScanResult {
+  uint32_t found_slab;  // slab holding the key (live or dead); valid if found_slot >= 0
+  int found_slot;
+  bool found_live;
+  uint32_t free_slab;  // first reusable slot in chain order; valid if free_slot >= 0
+  int free_slot;
+  uint32_t tail;       // last slab of the chain
+};
+
+template <class Tr>
+__device__ __forceinline__ bool scan_chain(const TableView& t, typename Tr::Key key, uint64_t h,
+                                           ScanResult& r, uint32_t start) {
+  const uint32_t fp = fingerprint(h);
+  const uint32_t live4 = (0x80u | fp) * 0x01010101u;
+  const uint32_t dead4 = fp * 0x01010101u;
+  uint32_t s = start;
+  for (uint32_t hop = 0; hop < kMaxHops; ++hop) {
+    const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
+    Meta m = load_meta(slab);
+    uint32_t live = tag_match(m, live4);
+    uint32_t cand = live | tag_match(m, dead4);
+    while (cand) {
+      int slot = __ffs(cand) - 1;
+      cand &= cand - 1;
+      if (key_load<Tr>(slab + kMetaBytes + slot * Tr::kSlotBytes) == key) {
+        r.found_slab = s;
+        r.found_slot = slot;
+        r.found_live = (live >> slot) & 1u;
+        r.tail = s;
+        return true;
+      }
+    }
+    if (r.free_slot < 0) {
+      uint32_t fr = tag_match(m, 0u);  // empty
+      if constexpr (Tr::kReuseDead) {
+        // dead tags: nonzero with the top bit clear
+#pragma unroll
+        for (int w = 0; w < 7; ++w) {
+          uint32_t x = m.tag[w];
+          uint32_t nz = ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x;  // top bit set iff byte != 0
+          uint32_t dead = nz & ~x & 0x80808080u;                // nonzero and top bit clear
+          uint32_t b = (dead >> 7) & 0x01010101u;
+          b = (b | (b >> 7));
+          b = (b | (b >> 14)) & 0xFu;
+          fr |= b << (4 * w);
+        }
+      }
+      fr &= (1u << kSlots) - 1u;
+      if (fr) {
+        r.free_slab = s;
+        r.free_slot = __ffs(fr) - 1;
+      }
+    }
+    r.tail = s;
+    if (m.next == 0) return false;
+    s = m.next;
+  }
+  raise_status(t.status, kStatusChain);
+  return false;
+}
+
+__device__ __forceinline__ uint32_t* tag_word(uint8_t* slab, int slot) {
+  return (uint32_t*)(slab + 4 + 4 * (slot >> 2));
+}
+
+template <class Tr>
+__device__ void table_apply_locked(const TableView& t, typename Tr::Key key, uint64_t h,
+                                   bool present, uint64_t val) {
+  const uint32_t bucket = (uint32_t)h & t.mask;
+  if (!lock_writer(t, bucket)) return;
+  const uint32_t fp = fingerprint(h);
+  ScanResult r;
+  r.found_slot = -1;
+  r.free_slot = -1;
+  bool found = scan_chain<Tr>(t, key, h, r, bucket);
+  if (found) {
+    uint8_t* slab = slab_ptr(t.slabs, r.found_slab, Tr::kSlabBytes);
+    uint8_t* tagp = slab + 4 + r.found_slot;
+    if (present) {
+      if constexpr (Tr::kHasValue)
+        st_cg_u64(slab + kMetaBytes + r.found_slot * Tr::kSlotBytes + 8, val);
+      if (!r.found_live) {
+        __threadfence();
+        st_cg_u8(tagp, (uint8_t)(0x80u | fp));
+      }
+    } else if (r.found_live) {
+      st_cg_u8(tagp, (uint8_t)fp);
+    }
+  } else if (present) {
+    if (r.free_slot >= 0) {
+      uint8_t* slab = slab_ptr(t.slabs, r.free_slab, Tr::kSlabBytes);
+      key_store<Tr>(slab + kMetaBytes + r.free_slot * Tr::kSlotBytes, key, val);
+      __threadfence();
+      st_cg_u8(slab + 4 + r.free_slot, (uint8_t)(0x80u | fp));
+    } else {
+      uint32_t n = pool_alloc(t);
+      if (n != 0) {
+        uint8_t* slab = slab_ptr(t.slabs, n, Tr::kSlabBytes);
+        key_store<Tr>(slab + kMetaBytes, key, val);
+        st_cg_u8(slab + 4, (uint8_t)(0x80u | fp));
+        __threadfence();
+        st_cg_u32(slab_ptr(t.slabs, r.tail, Tr::kSlabBytes), n);
+      }
+    }
+  }
+  unlock_writer(t, bucket);
+}
+
+template <class Tr>
+__device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, uint64_t h,
+                                     bool present, uint64_t val) {
+  const uint32_t bucket = (uint32_t)h & t.mask;
+  const uint32_t fp = fingerprint(h);
+  uint32_t spare = 0;  // slab taken from the pool but not linked yet
+  uint32_t start = bucket;
+  for (uint32_t attempt = 0; attempt < kLockPolls; ++attempt) {
+    ScanResult r;
+    r.found_slot = -1;
+    r.free_slot = -1;
+    bool found = scan_chain<Tr>(t, key, h, r, start);
+    if (found) {
+      uint8_t* slab = slab_ptr(t.slabs, r.found_slab, Tr::kSlabBytes);
+      uint32_t* tw = tag_word(slab, r.found_slot);
+      const uint32_t sh = 8 * (r.found_slot & 3);
+      if (present) {
+        if constexpr (Tr::kHasValue)
+          st_cg_u64(slab + kMetaBytes + r.found_slot * Tr::kSlotBytes + 8, val);
+        if (!r.found_live) {
+          __threadfence();
+          atomicOr(tw, 0x80u << sh);
+        }
+      } else if (r.found_live) {
+        atomicAnd(tw, ~(0x80u << sh));
+      }
+      return;  // the spare (if any) stays unlinked: at most one slab lost per race
+    }
+    if (!present) return;
+    if (r.free_slot >= 0) {
+      uint8_t* slab = slab_ptr(t.slabs, r.free_slab, Tr::kSlabBytes);
+      uint32_t* tw = tag_word(slab, r.free_slot);
+      const uint32_t sh = 8 * (r.free_slot & 3);
+      uint32_t cur = ld_cg_u32(tw);
+      uint32_t byte = (cur >> sh) & 0xFFu;
+      bool reusable = (byte == 0) || (Tr::kReuseDead && byte != 0x80u && !(byte & 0x80u));
+      if (reusable) {
+        uint32_t claimed = (cur & ~(0xFFu << sh)) | (0x80u << sh);
+        if (atomicCAS(tw, cur, claimed) == cur) {
+          key_store<Tr>(slab + kMetaBytes + r.free_slot * Tr::kSlotBytes, key, val);
+          __threadfence();
+          atomicXor(tw, (0x80u ^ (0x80u | fp)) << sh);  // busy -> live
+          return;
+        }
+      }
+      start = bucket;  // lost the race: rescan from the head
+      continue;
+    }
+    if (spare == 0) {
+      spare = pool_alloc(t);
+      if (spare == 0) return;  // OOM raised
+      uint8_t* slab = slab_ptr(t.slabs, spare, Tr::kSlabBytes);
+      key_store<Tr>(slab + kMetaBytes, key, val);
+      st_cg_u8(slab + 4, (uint8_t)(0x80u | fp));
+      __threadfence();
+    }
+    uint32_t* link = (uint32_t*)slab_ptr(t.slabs, r.tail, Tr::kSlabBytes);
+    if (atomicCAS(link, 0u, spare) == 0u) return;
+    // Someone linked a slab first.  The spare (holding only this key) stays
+    // ours for a later link attempt; if a free slot turns up instead it is
+    // never linked and is lost (at most one slab per lost race).
+    start = bucket;
+  }
+  raise_status(t.status, kStatusTimeout);
+}
+
+template <class Tr>
+__device__ __forceinline__ void table_apply(const TableView& t, typename Tr::Key key, uint64_t h,
+                                            bool present, uint64_t val) {
+  if (t.lock_mode == kLockFree)
+    table_apply_lockfree<Tr>(t, key, h, present, val);
+  else
+    table_apply_locked<Tr>(t, key, h, present, val);
+}
+
+// -------------------------------------------------------- grid barrier
+// Sense-counting barrier for a cooperative (co-resident) grid.  Each wait
+// polls at most kBarrierPolls times; on timeout it raises kStatusBarrier and
+// returns false so the caller can leave the kernel.
+struct GridBarrier {
+  uint32_t count;
+  uint32_t gen;
+};
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    uint32_t g = ld_acquire_u32(&b->gen);
+    __threadfence();
+    if (atomicAdd(&b->count, 1u) == nblocks - 1) {
+      b->count = 0;
+      __threadfence();
+      st_release_u32(&b->gen, g + 1);
+    } else {
+      uint32_t it = 0;
+      while (ld_acquire_u32(&b->gen) == g) {
+        if (++it > kBarrierPolls || (*(volatile uint32_t*)status & kStatusBarrier)) {
+          raise_status(status, kStatusBarrier);
+          ok = 0;
+          break;
+        }
+        __nanosleep(it < 64 ? 20 : 200);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+}  // namespace lsb

@@ -1,0 +1,255 @@
+"""GPU parity of the map against the oracle (lslab's slab list restated on the
+host, run in op-index order).  Integer results must be bit-exact."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from lslab_b200 import Map, LsbError, STATUS_OOM, OP_GET, OP_PUT, OP_REMOVE
+from lslab_b200 import workload as W
+from oracle import OracleMap
+from tests.util import dev, host, results, results_buf, same_results, first_mismatch
+
+pytestmark = pytest.mark.gpu
+
+
+def _sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def test_get_put_known_answer(cuda):
+    """test/slabunified_test.cu:42-89: put keys 1..1024 with value rep returns
+    rep-1; get returns {true, rep}; 100 reps on 2^10 buckets."""
+    m = Map(10)
+    keys = dev(np.arange(1, 1025, dtype=np.uint64))
+    old = cuda.zeros(1024, dtype=cuda.int64, device="cuda")
+    out = results_buf(1024)
+    for rep in range(100):
+        vals = dev(np.full(1024, rep, np.uint64))
+        m.put(keys, vals, old)
+        m.get(keys, out)
+        _sync()
+        if rep:
+            assert (host(old, np.uint64) == rep - 1).all()
+        r = results(out)
+        assert r["found"].all() and (r["value"] == rep).all()
+    assert m.status() == 0
+
+
+def test_small_plain_gets_vs_oracle(cuda):
+    """Plain-method shape at small size: insert distinct splitmix64 keys with
+    value = key ^ 0x9E3779B97F4A7C15, then gets half present, half absent."""
+    seed, log2, n = 11, 10, 1 << 14
+    pk = W.prefill_keys(seed, n)
+    pv = W.prefill_values(pk)
+    ak = W.absent_keys(seed, n, pk)
+    q = np.concatenate([pk[: n // 2], ak[: n // 2]])
+    q = q[np.argsort(W.splitmix64(seed + 99, 0, len(q)))]
+
+    o = OracleMap(log2)
+    o_old = o.put(pk, pv)
+    want = o.get(q)
+
+    m = Map(log2)
+    old = cuda.zeros(n, dtype=cuda.int64, device="cuda")
+    m.put(dev(pk), dev(pv), old)
+    out = results_buf(len(q))
+    m.get(dev(q), out)
+    _sync()
+    assert (host(old, np.uint64) == o_old).all()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)
+    assert m.status() == 0
+
+
+def _mixed_case(seed, n, key_space, mix=(0.5, 0.35, 0.15)):
+    u = W.uniform01(seed, 0, n)
+    cum = np.cumsum(mix)
+    types = np.searchsorted(cum[:-1], u, side="right").astype(np.uint8)
+    keys = W.key_of_rank(seed, (W.splitmix64(seed + 1, 0, n) % np.uint64(key_space)))
+    vals = W.splitmix64(seed + 2, 0, n)
+    return types, keys, vals
+
+
+@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("window", [0, 4096])
+def test_mixed_conflicts_vs_oracle(cuda, fused, window):
+    """Random get/put/remove order over a small key space (heavy same-key
+    conflicts inside and across windows): every result and the final contents
+    equal the sequential replay."""
+    n, log2 = 60_000, 6
+    types, keys, vals = _mixed_case(5, n, key_space=300)
+    o = OracleMap(log2)
+    want = o.mixed(types, keys, vals)
+    m = Map(log2, max_window=window)
+    out = results_buf(n)
+    run = m.execute_fused if fused else m.execute
+    run(dev(types), dev(keys), dev(vals), out)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)
+    assert m.status() == 0
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_hot_key_big_groups(cuda, fused):
+    """One key carries thousands of mutations in one window (block-wide sort
+    path) interleaved with reads of it and of other keys."""
+    n = 200_000
+    rng = np.random.default_rng(3)
+    types = rng.choice([OP_GET, OP_PUT, OP_REMOVE], size=n, p=[0.6, 0.3, 0.1]).astype(np.uint8)
+    keys = W.key_of_rank(9, rng.integers(0, 50, size=n))
+    keys[rng.random(n) < 0.5] = np.uint64(0xDEADBEEF)
+    vals = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
+    o = OracleMap(8)
+    want = o.mixed(types, keys, vals)
+    m = Map(8)
+    out = results_buf(n)
+    (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    assert m.status() == 0
+
+
+def test_type_sorted_batches_plain_equals_fused(cuda):
+    """The 95/5 Zipf workload shape at small size: per-op-type calls (gets then
+    puts) and the fused path give identical results, equal to the oracle."""
+    seed, log2, items = 21, 12, 1 << 16
+    pk = W.prefill_keys(seed, items)
+    pv = W.prefill_values(pk)
+    o = OracleMap(log2)
+    o.put(pk, pv)
+    a, b = Map(log2), Map(log2)
+    a.put(dev(pk), dev(pv))
+    b.put(dev(pk), dev(pv))
+    for bi in range(3):
+        bt = W.map_zipf_batch(seed, bi, 1 << 15, items, 0.99, (0.95, 0.05))
+        want = o.mixed(bt.types, bt.keys, bt.vals)
+        ng = int(np.sum(bt.types == OP_GET))
+        # plain: get launch then put launch
+        outg = results_buf(ng)
+        old = cuda.zeros(len(bt.keys) - ng, dtype=cuda.int64, device="cuda")
+        a.get(dev(bt.keys[:ng]), outg)
+        a.put(dev(bt.keys[ng:]), dev(bt.vals[ng:]), old)
+        # fused
+        outf = results_buf(len(bt.keys))
+        b.execute_fused(dev(bt.types), dev(bt.keys), dev(bt.vals), outf)
+        _sync()
+        gf = results(outf)
+        assert same_results(gf, want), first_mismatch(gf, want)
+        gg = results(outg)
+        assert same_results(gg, want[:ng]), first_mismatch(gg, want[:ng])
+        assert np.array_equal(host(old, np.uint64), want["value"][ng:])
+    ka, va = a.dump()
+    kb, vb = b.dump()
+    ko, vo = o.dump()
+    assert np.array_equal(ka, ko) and np.array_equal(va, vo)
+    assert np.array_equal(kb, ko) and np.array_equal(vb, vo)
+
+
+def test_remove_then_reinsert(cuda):
+    """Remove half, re-put some (same-key revival), get all; also the
+    AoS put form (map.h:189-192)."""
+    n, log2 = 20_000, 8
+    keys = W.prefill_keys(31, n)
+    vals = W.prefill_values(keys)
+    o = OracleMap(log2)
+    m = Map(log2)
+    pairs = np.stack([keys, vals], axis=1).reshape(-1)
+    old = cuda.zeros(n, dtype=cuda.int64, device="cuda")
+    m.put_pairs(dev(pairs), old)
+    o.put(keys, vals)
+    rk = keys[::2]
+    out = results_buf(len(rk))
+    m.remove(dev(rk), out)
+    want = o.remove(rk)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    again = keys[::4]
+    nv = W.splitmix64(77, 0, len(again))
+    old2 = cuda.zeros(len(again), dtype=cuda.int64, device="cuda")
+    m.put(dev(again), dev(nv), old2)
+    want_old = o.put(again, nv)
+    q = np.concatenate([keys, W.absent_keys(31, 1000, keys)])
+    outq = results_buf(len(q))
+    m.get(dev(q), outq)
+    wq = o.get(q)
+    _sync()
+    assert np.array_equal(host(old2, np.uint64), want_old)
+    gq = results(outq)
+    assert same_results(gq, wq), first_mismatch(gq, wq)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)
+
+
+def test_long_chains_and_edge_keys(cuda):
+    """Tiny bucket array so chains grow many slabs deep; keys 0 and 2^64-1 are
+    ordinary keys (no sentinel)."""
+    log2 = 2
+    keys = np.concatenate([np.array([0, 2**64 - 1], np.uint64), W.prefill_keys(41, 3000)])
+    vals = np.concatenate([np.array([0, 2**64 - 1], np.uint64), W.splitmix64(42, 0, 3000)])
+    o = OracleMap(log2)
+    m = Map(log2, pool_slabs=1024)
+    old = cuda.zeros(len(keys), dtype=cuda.int64, device="cuda")
+    m.put(dev(keys), dev(vals), old)
+    o.put(keys, vals)
+    out = results_buf(len(keys))
+    m.get(dev(keys), out)
+    _sync()
+    got = results(out)
+    want = o.get(keys)
+    assert same_results(got, want), first_mismatch(got, want)
+    used, cap = m.pool_usage()
+    assert used >= (len(keys) // 28) - 4 and cap == 1024
+    assert m.status() == 0
+
+
+def test_pool_exhaustion_reports_oom(cuda):
+    """A pool too small for the inserts: the device raises OOM in the status
+    word (the reference traps instead); nothing faults."""
+    m = Map(1, pool_slabs=2)
+    keys = W.prefill_keys(51, 2000)
+    m.put(dev(keys), dev(keys))
+    st = m.status()
+    assert st & STATUS_OOM
+    assert m.status() == 0  # cleared by the read
+
+
+@pytest.mark.parametrize("mode", ["free", "rw"])
+def test_lock_modes_agree(cuda, mode):
+    n, log2 = 40_000, 5
+    types, keys, vals = _mixed_case(61, n, key_space=2000)
+    o = OracleMap(log2)
+    want = o.mixed(types, keys, vals)
+    m = Map(log2, lock_mode=mode)
+    out = results_buf(n)
+    m.execute(dev(types), dev(keys), dev(vals), out)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)
+    assert m.status() == 0
+
+
+def test_empty_and_bad_arguments(cuda):
+    m = Map(4)
+    e = cuda.empty(0, dtype=cuda.int64, device="cuda")
+    m.get(e, results_buf(0), size=0)
+    m.put(e, e, None, size=0)
+    with pytest.raises(LsbError):
+        m.get(0, 0, size=5)  # null keys
+    with pytest.raises(LsbError):
+        Map(0)  # zero log2 buckets
+    assert m.buckets() == 16
