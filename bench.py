@@ -1,0 +1,585 @@
+"""Benchmark: batched get/put on map<uint64,uint64>, the headline workload.
+
+Workload (default): map with 2^22 buckets (table > L2), prefilled with 2^26
+splitmix64 keys (value = key ^ 0x9E3779B97F4A7C15); each step is one batch of
+2^20 ops, 95% get / 5% put, keys Zipf(0.99) over the 2^26 prefill keys, put
+values uniform u64; a batch is issued gets first, then puts (the order a
+per-op-type caller issues it).  Synthetic seeded data; every step uses a
+distinct batch.
+
+Arms:
+  ours (default)   `value`: the fused persistent kernel (lsb_map_execute_fused),
+                   inputs resident in HBM; `plain_value`: per-op-type launches
+                   (lsb_map_get then lsb_map_put) on an identical table, results
+                   checked bit-identical to the fused path; `e2e`: the fused call
+                   with pinned HOST buffers, H2D of the batch and D2H of the
+                   results inside the timed region.
+  --impl reference lslab's own kernels (map::get / map::put, built for sm_100a
+                   from the reference sources into oracle/_ref) on the same
+                   workload, per-op-type launches as the reference's API offers.
+
+Multi-GPU (torchrun, one rank per GPU): every rank owns an independent table
+shard and its own batch stream (weak scaling, no data-path collective); time is
+the max over ranks of the device-timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mops/s (95/5 get/put, Zipf 0.99) batched vs plain kernels; p50/p99 latency"
+BYTES_GET = 88   # request 8 + response 16 + key sector 32 + value sector 32
+BYTES_PUT = 120  # request 16 + response 8 + key sector 32 + value sector 32 + write-back 32
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--buckets-log2", type=int, default=22)
+    ap.add_argument("--prefill-log2", type=int, default=26)
+    ap.add_argument("--batch-log2", type=int, default=20)
+    ap.add_argument("--theta", type=float, default=0.99)
+    ap.add_argument("--put-frac", type=float, default=0.05)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--soak-s", type=float, default=1.0,
+                    help="untimed read-only load before timing so clocks leave idle")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-batches", type=int, default=4)
+    ap.add_argument("--cpu-seconds", type=float, default=3.0)
+    ap.add_argument("--lock-mode", default="writer", choices=["writer", "free", "rw"])
+    ap.add_argument("--block", type=int, default=0, help="threads per block (0 = library default)")
+    ap.add_argument("--prefetch", type=int, default=-1)
+    ap.add_argument("--chunk", type=int, default=-1)
+    ap.add_argument("--dedup", type=int, default=-1)
+    ap.add_argument("--split", type=int, default=-1, help="fused: percent of reads probed first")
+    ap.add_argument("--trace", action="store_true", help="single mode: print fused phase times")
+    ap.add_argument("--single", action="store_true",
+                    help="fused timing only (one table, no plain/e2e/cpu legs): the small "
+                         "case for profiler captures")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        loaded = [r for r in rows if r[2] > 0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in loaded for j, v in enumerate(r[3]) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded)}
+
+
+def dev_u64(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.int64)).cuda()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(name: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/<name>.txt, line 'dram_bytes_per_launch: N'), or None."""
+    p = ROOT / "profiles" / f"{name}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ workload
+def make_batches(args, rank: int, count: int):
+    from lslab_b200 import workload as W
+    seed = args.seed + 1000 * rank
+    n = 1 << args.batch_log2
+    items = 1 << args.prefill_log2
+    return [W.map_zipf_batch(seed, b, n, items, args.theta, (1 - args.put_frac, args.put_frac))
+            for b in range(count)]
+
+
+def prefill_arrays(args, rank: int):
+    from lslab_b200 import workload as W
+    seed = args.seed + 1000 * rank
+    keys = W.prefill_keys(seed, 1 << args.prefill_log2)
+    return keys, W.prefill_values(keys)
+
+
+def alg_bytes(batch) -> float:
+    nput = int(np.sum(batch.types == 1))
+    return (len(batch.keys) - nput) * BYTES_GET + nput * BYTES_PUT
+
+
+def apply_tuning(args, table):
+    kw = {}
+    if args.block:
+        kw["block_threads"] = args.block
+    if args.prefetch >= 0:
+        kw["prefetch"] = args.prefetch
+    if args.chunk >= 0:
+        kw["chunk"] = args.chunk
+    if args.dedup >= 0:
+        kw["dedup"] = args.dedup
+    if args.split >= 0:
+        kw["fused_split"] = args.split
+    if kw:
+        table.set_tuning(**kw)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, world, rank, local):
+    import torch
+    import lslab_b200 as L
+
+    stream = torch.cuda.current_stream()
+    n = 1 << args.batch_log2
+    nb = args.warmup + args.steps
+    batches = make_batches(args, rank, nb)
+    pk, pv = prefill_arrays(args, rank)
+    pool = max(1 << (args.buckets_log2 - 2), 4096)
+    fused = L.Map(args.buckets_log2, pool, lock_mode=args.lock_mode)
+    plain = fused if args.single else L.Map(args.buckets_log2, pool, lock_mode=args.lock_mode)
+    apply_tuning(args, fused)
+    apply_tuning(args, plain)
+    for off in range(0, len(pk), 1 << 24):
+        k = dev_u64(torch, pk[off:off + (1 << 24)])
+        v = dev_u64(torch, pv[off:off + (1 << 24)])
+        fused.put(k, v)
+        if not args.single:
+            plain.put(k, v)
+        del k, v
+    torch.cuda.synchronize()
+    st = fused.status() | plain.status()
+    assert st == 0, f"prefill raised device status {st:#x}"
+
+    d_types = [torch.from_numpy(b.types).cuda() for b in batches]
+    d_keys = [dev_u64(torch, b.keys) for b in batches]
+    d_vals = [dev_u64(torch, b.vals) for b in batches]
+    n_get = [int(np.sum(b.types == 0)) for b in batches]
+    out_f = [torch.empty((n, 2), dtype=torch.int64, device="cuda") for _ in range(nb)]
+    if args.single:
+        ops = n * args.steps
+        for b in range(args.warmup):
+            fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for s in range(args.steps):
+            b = args.warmup + s
+            fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        phases = None
+        if args.trace:
+            fused.set_trace(True)
+            b = args.warmup
+            fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+            tr = fused.read_trace()
+            phases = [round((tr[k + 1][0] - tr[k][0]) / 1e3, 2) for k in range(len(tr) - 1)]
+        if rank == 0:
+            print(json.dumps({"single": True, "phases_us": phases, "value": round(ops / (ms * 1e-3) / 1e6, 2),
+                              "unit": "Mops/s", "ms_per_step": round(ms / args.steps, 5),
+                              "tuning": fused.tuning(),
+                              "device_status": fused.status()}), flush=True)
+        return
+    out_g = [torch.empty((n, 2), dtype=torch.int64, device="cuda") for _ in range(nb)]
+    out_p = [torch.empty(n - n_get[b], dtype=torch.int64, device="cuda") for b in range(nb)]
+
+    clocks = Clocks(local)
+    # soak (untimed, read-only so both tables stay identical): gets of the
+    # batch keys until soak_s has passed, so clocks have left idle
+    t_end = time.perf_counter() + args.soak_s
+    i = 0
+    while time.perf_counter() < t_end:
+        fused.get(d_keys[i % nb], out_f[i % nb])
+        i += 1
+        if i % 50 == 0:
+            torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    # warm-up (untimed): W fused steps
+    for b in range(args.warmup):
+        fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+    torch.cuda.synchronize()
+
+    # ---- timed: fused
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier(world)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for s in range(args.steps):
+        b = args.warmup + s
+        fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+        ev[s + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [ev[s].elapsed_time(ev[s + 1]) for s in range(args.steps)]
+    fused_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), world)
+
+    # ---- plain per-op-type launches on an identical table
+    for b in range(args.warmup):
+        g = n_get[b]
+        plain.get(d_keys[b][:g], out_g[b])
+        plain.put(d_keys[b][g:], d_vals[b][g:], out_p[b])
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    pe0.record(stream)
+    for s in range(args.steps):
+        b = args.warmup + s
+        g = n_get[b]
+        plain.get(d_keys[b][:g], out_g[b])
+        plain.put(d_keys[b][g:], d_vals[b][g:], out_p[b])
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    plain_ms = max_over_ranks(pe0.elapsed_time(pe1), world)
+
+    # identical results: fused out == plain (get part, then put old values)
+    identical = True
+    for b in range(nb):
+        g = n_get[b]
+        f = out_f[b]
+        if not torch.equal(f[:g], out_g[b][:g]) or not torch.equal(f[g:, 1], out_p[b]):
+            identical = False
+            break
+    st = fused.status() | plain.status()
+
+    # ---- e2e through the public API with host buffers
+    h_types = [torch.from_numpy(b.types).pin_memory() for b in batches]
+    h_keys = [torch.from_numpy(b.keys.view(np.int64)).pin_memory() for b in batches]
+    h_vals = [torch.from_numpy(b.vals.view(np.int64)).pin_memory() for b in batches]
+    h_out = torch.empty((n, 2), dtype=torch.int64).pin_memory()
+    s_types = torch.empty(n, dtype=torch.uint8, device="cuda")
+    s_keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    s_vals = torch.empty(n, dtype=torch.int64, device="cuda")
+    s_out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+
+    def e2e_step(b):
+        s_types.copy_(h_types[b], non_blocking=True)
+        s_keys.copy_(h_keys[b], non_blocking=True)
+        s_vals.copy_(h_vals[b], non_blocking=True)
+        fused.execute_fused(s_types, s_keys, s_vals, s_out)
+        h_out.copy_(s_out, non_blocking=True)
+
+    for b in range(args.warmup):
+        e2e_step(b)
+    torch.cuda.synchronize()
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ee0.record(stream)
+    for s in range(args.steps):
+        e2e_step(args.warmup + s)
+    ee1.record(stream)
+    torch.cuda.synchronize()
+    wall_e2e = time.perf_counter() - t0
+    barrier(world)
+    e2e_ms = max_over_ranks(ee0.elapsed_time(ee1), world)
+
+    clk = clocks.stop()
+    st |= fused.status()
+
+    ops_rank = n * args.steps
+    ops_total = ops_rank * world
+    value = ops_total / (fused_ms * 1e-3) / 1e6
+    plain_value = ops_total / (plain_ms * 1e-3) / 1e6
+    e2e_value = ops_total / (e2e_ms * 1e-3) / 1e6
+    ab = [alg_bytes(batches[args.warmup + s]) for s in range(args.steps)]
+    per_launch_s = statistics.mean(step_ms) * 1e-3
+    achieved = statistics.mean(ab) / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = profiled_traffic("fused_map_cfg2")
+
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mops/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(fused_ms / args.steps, 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded splitmix64 keys, Zipf 0.99 ranks)",
+        "config": {
+            "workload": (f"map<u64,u64> 2^{args.buckets_log2} buckets prefilled with "
+                         f"2^{args.prefill_log2} keys; batches of 2^{args.batch_log2} ops, "
+                         f"{100 - 100 * args.put_frac:.0f}/{100 * args.put_frac:.0f} get/put, "
+                         f"Zipf {args.theta} over the prefill keys, gets then puts per batch"),
+            "buckets_log2": args.buckets_log2,
+            "prefill_log2": args.prefill_log2,
+            "batch_ops": n,
+            "form": "fused persistent kernel (value); per-op-type launches (plain_value)",
+            "lock_mode": args.lock_mode,
+            "tuning": fused.tuning(),
+            "l2": ("no flush: table 2^%d x 480 B = %.1f GB > L2; each step a distinct batch"
+                   % (args.buckets_log2, (1 << args.buckets_log2) * 480 / 1e9)),
+            "parallelism": f"{world} independent table shard(s), one per GPU",
+        },
+        "plain_value": round(plain_value, 2),
+        "fused_over_plain": round(value / plain_value, 3),
+        "results_identical_fused_vs_plain": identical,
+        "device_status": st,
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mops/s",
+                "h2d_bytes_per_step": int(n * 17), "d2h_bytes_per_step": int(n * 16),
+                "wall_s": round(wall_e2e, 4)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
+                     "alg_bytes_per_op": round(statistics.mean(ab) / n, 2)},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, batches)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args, batches):
+    """The oracle (plain-C restatement of the reference's slab list) replaying
+    a bounded sample of the same workload on the host cores, bucket-sharded
+    over threads (results identical to the sequential replay)."""
+    from oracle import OracleMap
+    threads = max(1, min(32, os.cpu_count() or 1))
+    pk, pv = prefill_arrays(args, 0)
+    o = OracleMap(args.buckets_log2, 1 << 16)
+    chunk = 1 << 22
+    put_t = np.ones(chunk, np.uint8)
+    for off in range(0, len(pk), chunk):
+        k = pk[off:off + chunk]
+        o.mixed(put_t[:len(k)], k, pv[off:off + chunk], threads=threads)
+    nb = min(args.cpu_batches, len(batches))
+    t0 = time.perf_counter()
+    ops = 0
+    reps = 0
+    while True:  # cycle the sample batches for at least cpu_seconds of wall time
+        for b in batches[:nb]:
+            o.mixed(b.types, b.keys, b.vals, threads=threads)
+            ops += len(b.keys)
+        reps += 1
+        if time.perf_counter() - t0 >= args.cpu_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(ops / dt / 1e6, 2), "unit": "Mops/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{nb} batches of {len(batches[0].keys)} ops replayed {reps}x "
+                      f"({ops} ops) on the full-size table (2^{args.buckets_log2} buckets, "
+                      f"2^{args.prefill_log2} prefill): {dt:.2f} s wall on {threads} threads"}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, world, rank, local):
+    import torch
+    import oracle
+    from oracle import RefMap, ref_map_pool_bound
+
+    if rank != 0:
+        return  # rank 0 alone runs the reference arm
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/liblslab_ref.so not built"}))
+        return
+    stream = torch.cuda.current_stream()
+    n = 1 << args.batch_log2
+    nb = args.warmup + args.steps
+    batches = make_batches(args, 0, nb)
+    pk, pv = prefill_arrays(args, 0)
+    inserts = np.concatenate([pk] + [b.keys[b.types == 1] for b in batches])
+    pool = ref_map_pool_bound(args.buckets_log2, inserts)
+    del inserts
+    m = RefMap(args.buckets_log2, pool)
+    for off in range(0, len(pk), 1 << 22):
+        k = dev_u64(torch, pk[off:off + (1 << 22)])
+        v = dev_u64(torch, pv[off:off + (1 << 22)])
+        old = torch.empty_like(k)
+        m.put(k, v, old, stream.cuda_stream)
+    torch.cuda.synchronize()
+    d_keys = [dev_u64(torch, b.keys) for b in batches]
+    d_vals = [dev_u64(torch, b.vals) for b in batches]
+    n_get = [int(np.sum(b.types == 0)) for b in batches]
+    out_g = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    out_p = torch.empty(n, dtype=torch.int64, device="cuda")
+
+    def step(b, keys, vals):
+        g = n_get[b]
+        m.get(keys[:g], out_g[:g], stream.cuda_stream)
+        m.put(keys[g:], vals[g:], out_p[: n - g], stream.cuda_stream)
+
+    clocks = Clocks(local)
+    for b in range(args.warmup):
+        step(b, d_keys[b], d_vals[b])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(args.steps):
+        b = args.warmup + s
+        step(b, d_keys[b], d_vals[b])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+
+    # e2e: host buffers, copies inside the timed region
+    h_keys = [torch.from_numpy(b.keys.view(np.int64)).pin_memory() for b in batches]
+    h_vals = [torch.from_numpy(b.vals.view(np.int64)).pin_memory() for b in batches]
+    h_out = torch.empty((n, 2), dtype=torch.int64).pin_memory()
+    h_old = torch.empty(n, dtype=torch.int64).pin_memory()
+    s_keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    s_vals = torch.empty(n, dtype=torch.int64, device="cuda")
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for s in range(args.steps):
+        b = args.warmup + s
+        s_keys.copy_(h_keys[b], non_blocking=True)
+        s_vals.copy_(h_vals[b], non_blocking=True)
+        step(b, s_keys, s_vals)
+        g = n_get[b]
+        h_out[:g].copy_(out_g[:g], non_blocking=True)
+        h_old[: n - g].copy_(out_p[: n - g], non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    clk = clocks.stop()
+    value = n * args.steps / (ms * 1e-3) / 1e6
+    e2e_value = n * args.steps / (e2e_ms * 1e-3) / 1e6
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mops/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded splitmix64 keys, Zipf 0.99 ranks)",
+        "config": {
+            "workload": (f"map<u64,u64> 2^{args.buckets_log2} buckets prefilled with "
+                         f"2^{args.prefill_log2} keys; batches of 2^{args.batch_log2} ops, "
+                         f"{100 - 100 * args.put_frac:.0f}/{100 * args.put_frac:.0f} get/put, "
+                         f"Zipf {args.theta} over the prefill keys, gets then puts per batch"),
+            "form": "lslab map::get<256> then map::put<256> per batch (its only batched form)",
+        },
+        "reference": ("depaulmillz/lslab's own map kernels built for sm_100a from its headers; "
+                      "the reference has no CPU implementation of this path"),
+        "cpu_baseline": {"value": round(value, 2), "unit": "Mops/s", "cores": 0,
+                         "kind": "reference",
+                         "sample": (f"{args.steps} batches of {n} ops on the GPU (the reference "
+                                    "is GPU-only; no host cores do the work)")},
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mops/s", "h2d_bytes_per_step": n * 16,
+                "d2h_bytes_per_step": int(statistics.mean(16 * g + 8 * (n - g) for g in n_get))},
+        "pool_slabs_used": m.pool_used(),
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

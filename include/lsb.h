@@ -82,6 +82,18 @@ typedef struct lsb_options {
   int device;            /* CUDA device; -1 = current                            */
 } lsb_options;
 
+/* Launch tuning of a table (see lsb_*_set_tuning); the autotuner picks it. */
+typedef struct lsb_tuning {
+  uint32_t block_threads; /* threads per block: 128, 256, 512 or 1024 (4..32 warps) */
+  uint32_t chunk;         /* ops a block claims per step in the probe phase (its warps
+                             share them out), multiple of 32 up to 2^20; 0 = static
+                             grid stride */
+  uint32_t prefetch;      /* extra lookups a thread keeps in flight: 0, 1 or 2 */
+  uint32_t dedup;         /* 1: lanes of a warp carrying the same key share one lookup */
+  uint32_t fused_split;   /* fused path: percent of a window's reads probed before the
+                             same-key ordering pass (the rest run during it), 0..100 */
+} lsb_tuning;
+
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */
 #define LSB_LOCK_FREE 1u     /* writers claim slots with CAS on slab words, no lock   */
 #define LSB_LOCK_RW 2u       /* reference-style: readers take a shared bucket lock too */
@@ -133,6 +145,22 @@ int lsb_map_execute_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys
 /* lslab::map::buckets(), include/lslab/map.h:225-227. */
 uint32_t lsb_map_buckets(const lsb_map* m);
 
+/* Launch tuning (no reference counterpart: the reference fixes the launch as a
+ * template block size, include/lslab/map.h:189-220). */
+int lsb_map_get_tuning(const lsb_map* m, lsb_tuning* out);
+int lsb_map_set_tuning(lsb_map* m, const lsb_tuning* t);
+
+/* Phase tracing of the fused path (no reference counterpart; the reference
+ * only brackets whole launches with cudaProfilerStart/Stop,
+ * benchmark/benchmark.cu:91,119).  With tracing on, each fused launch records
+ * one %globaltimer stamp per phase boundary per window: entry = ns << 8 |
+ * (window & 63) << 2 | phase, phase 0 window start, 1 probe done, 2 ordering
+ * done, 3 resolve done.  read_trace copies the last launch's entries to host
+ * memory (synchronises the stream). */
+int lsb_map_set_trace(lsb_map* m, int on);
+int lsb_map_read_trace(lsb_map* m, uint64_t* out, size_t cap, size_t* count,
+                       cudaStream_t stream);
+
 /* Device status bits seen since the last call (synchronises the stream),
  * then clears them. */
 int lsb_map_status(lsb_map* m, uint32_t* flags, cudaStream_t stream);
@@ -177,6 +205,11 @@ int lsb_set_execute_fused(lsb_set* s, const uint8_t* types, const uint32_t* keys
                           size_t n, cudaStream_t stream);
 
 uint32_t lsb_set_buckets(const lsb_set* s); /* lslab::set::buckets(), set.h:361-363 */
+int lsb_set_get_tuning(const lsb_set* s, lsb_tuning* out);
+int lsb_set_set_tuning(lsb_set* s, const lsb_tuning* t);
+int lsb_set_set_trace(lsb_set* s, int on);
+int lsb_set_read_trace(lsb_set* s, uint64_t* out, size_t cap, size_t* count,
+                       cudaStream_t stream);
 int lsb_set_status(lsb_set* s, uint32_t* flags, cudaStream_t stream);
 int lsb_set_pool_usage(lsb_set* s, uint64_t* used, uint64_t* capacity, cudaStream_t stream);
 int lsb_set_size(lsb_set* s, uint64_t* count, cudaStream_t stream);

@@ -134,6 +134,28 @@ class _Table:
         self._call("size", C.byref(v), _stream(stream))
         return int(v.value)
 
+    def set_trace(self, on: bool = True) -> None:
+        self._call("set_trace", int(bool(on)))
+
+    def read_trace(self, stream=None) -> list[tuple[int, int, int]]:
+        """Phase stamps of the last fused launch: (ns, window, phase)."""
+        import numpy as np
+        buf = np.zeros(1024, np.uint64)
+        n = C.c_size_t()
+        self._call("read_trace", buf.ctypes.data, len(buf), C.byref(n), _stream(stream))
+        return [(int(x) >> 8, (int(x) >> 2) & 0x3F, int(x) & 3) for x in buf[: n.value]]
+
+    def tuning(self) -> dict:
+        t = _lib.Tuning()
+        self._call("get_tuning", C.byref(t))
+        return {f: int(getattr(t, f)) for f, _ in _lib.Tuning._fields_}
+
+    def set_tuning(self, **kw) -> None:
+        cur = self.tuning()
+        cur.update(kw)
+        t = _lib.Tuning(**cur)
+        self._call("set_tuning", C.byref(t))
+
 
 class Map(_Table):
     """map<uint64_t, uint64_t> (include/lslab/map.h:24-234)."""

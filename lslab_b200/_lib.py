@@ -50,6 +50,16 @@ class Options(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("block_threads", C.c_uint32),
+        ("chunk", C.c_uint32),
+        ("prefetch", C.c_uint32),
+        ("dedup", C.c_uint32),
+        ("fused_split", C.c_uint32),
+    ]
+
+
 _lib: C.CDLL | None = None
 
 _P = C.c_void_p
@@ -69,6 +79,10 @@ _SIGS = {
     "lsb_map_execute": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_execute_fused": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_buckets": (_U32, [_P]),
+    "lsb_map_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lsb_map_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lsb_map_set_trace": (C.c_int, [_P, C.c_int]),
+    "lsb_map_read_trace": (C.c_int, [_P, _P, _SZ, C.POINTER(_SZ), _P]),
     "lsb_map_status": (C.c_int, [_P, C.POINTER(_U32), _P]),
     "lsb_map_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
     "lsb_map_size": (C.c_int, [_P, C.POINTER(_U64), _P]),
@@ -82,6 +96,10 @@ _SIGS = {
     "lsb_set_execute": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
     "lsb_set_execute_fused": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
     "lsb_set_buckets": (_U32, [_P]),
+    "lsb_set_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lsb_set_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "lsb_set_set_trace": (C.c_int, [_P, C.c_int]),
+    "lsb_set_read_trace": (C.c_int, [_P, _P, _SZ, C.POINTER(_SZ), _P]),
     "lsb_set_status": (C.c_int, [_P, C.POINTER(_U32), _P]),
     "lsb_set_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
     "lsb_set_size": (C.c_int, [_P, C.POINTER(_U64), _P]),

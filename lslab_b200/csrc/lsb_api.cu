@@ -18,8 +18,7 @@ namespace {
 
 constexpr uint32_t kDefaultWindow = 1u << 20;
 constexpr uint32_t kMaxWindow = 1u << 23;  // owner field of a group slot is 24 bits
-constexpr int kPlainBlock = 256;
-constexpr int kFusedBlock = 512;
+constexpr uint32_t kTraceCap = 1024;        // phase-trace entries per fused launch
 
 // Device arrays must be naturally aligned for their element type; a
 // misaligned device access would fault the context, so it is refused here.
@@ -32,32 +31,24 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
   } while (0)
 
 // ------------------------------------------------------------- kernels
-template <class Tr, bool kGroup, bool kDedup>
-__global__ void __launch_bounds__(kPlainBlock) k_probe(TableView t, Scratch sc, Window<Tr> w) {
+// Every kernel is bounded to 64 registers a thread (launch bound 1024), so any
+// block size from 128 to 1024 threads can reach 2048 threads per SM.
+template <class Tr, bool kGroup, int P>
+__global__ void __launch_bounds__(1024, 1)
+    k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  phase_probe<Tr, kGroup, kDedup>(t, sc, w, warp, nwarps);
+  phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
 }
 
 template <class Tr>
-__global__ void __launch_bounds__(kPlainBlock) k_segments(Scratch sc, Window<Tr> w) {
-  phase_segments<Tr>(sc, w, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
-}
-
-template <class Tr>
-__global__ void __launch_bounds__(kPlainBlock) k_scatter(Scratch sc, Window<Tr> w) {
-  phase_scatter<Tr>(sc, w, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
-}
-
-template <class Tr>
-__global__ void __launch_bounds__(kPlainBlock) k_sort(Scratch sc, Window<Tr> w) {
+__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w) {
   extern __shared__ uint32_t smem[];
-  phase_sort_small<Tr>(sc, w, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
   phase_sort_big<Tr>(sc, w, smem);
 }
 
 template <class Tr>
-__global__ void __launch_bounds__(kPlainBlock) k_resolve(TableView t, Scratch sc, Window<Tr> w) {
+__global__ void __launch_bounds__(1024, 1) k_resolve(TableView t, Scratch sc, Window<Tr> w) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
   phase_resolve_reads<Tr>(sc, w, tid, nt);
@@ -70,17 +61,32 @@ struct FusedJob {
   Window<Tr> base;  // whole batch; n = total ops
   uint32_t window;  // ops per window
   uint32_t epoch0;  // epoch of the first window
+  uint32_t chunk;   // probe work claim size (0 = static stride)
+  uint32_t dedup;
+  uint32_t split_q16;  // fraction of reads probed with the mutations (x 65536)
+  uint64_t* trace;     // optional: phase-boundary timestamps (ns), block 0 records
 };
 
-template <class Tr>
-__global__ void __launch_bounds__(kFusedBlock, 2)
+// Phase trace: entry = globaltimer ns << 8 | window & 0x3F << 2 | phase (0 start,
+// 1 after probe, 2 after sort, 3 after resolve).  Block 0, thread 0 only.
+__device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t wi, uint32_t ph) {
+  if (tr == nullptr || blockIdx.x != 0 || threadIdx.x != 0 || at >= kTraceCap) return;
+  uint64_t ns;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns));
+  tr[at++] = (ns << 8) | ((uint64_t)(wi & 0x3F) << 2) | ph;
+}
+
+template <class Tr, int P>
+__global__ void __launch_bounds__(1024, 1)
     k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
   const uint32_t nblocks = gridDim.x;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   const uint32_t warp = tid >> 5, nwarps = nt >> 5;
   const uint32_t nwin = (job.base.n + job.window - 1) / job.window;
+  uint32_t tat = 0, seq = 0;
   for (uint32_t wi = 0; wi < nwin; ++wi) {
+    trace_mark(job.trace, tat, wi, 0);
     Window<Tr> w = job.base;
     const uint32_t start = wi * job.window;
     w.n = min(job.window, job.base.n - start);
@@ -93,19 +99,38 @@ __global__ void __launch_bounds__(kFusedBlock, 2)
     }
     w.epoch = job.epoch0 + wi;
     w.cnt = &sc.cnt[wi & 1];
+    // the other counter set was last read in window wi-1, which has ended
     if (tid == 0) win_counters_reset(&sc.cnt[(wi + 1) & 1]);
-    phase_probe<Tr, true, true>(t, sc, w, warp, nwarps);
-    if (!grid_barrier(bar, nblocks, t.status)) return;
-    phase_segments<Tr>(sc, w, tid, nt);
-    if (!grid_barrier(bar, nblocks, t.status)) return;
-    phase_scatter<Tr>(sc, w, tid, nt);
-    if (!grid_barrier(bar, nblocks, t.status)) return;
-    phase_sort_small<Tr>(sc, w, tid, nt);
-    phase_sort_big<Tr>(sc, w, smem);
-    if (!grid_barrier(bar, nblocks, t.status)) return;
-    phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
-    phase_resolve_reads<Tr>(sc, w, tid, nt);
-    if (!grid_barrier(bar, nblocks, t.status)) return;
+    // Reads [0, split) are probed with the mutations; reads [split, n) in the
+    // sort pass, where they fill the SMs that the (latency-bound, few-block)
+    // ordering of big groups leaves idle.  Reads do not depend on the groups.
+    const uint32_t split = (uint32_t)(((uint64_t)w.n * job.split_q16) >> 16);
+    phase_probe<Tr, true, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, job.chunk,
+                             job.dedup != 0, ProbeSel{0, split, true});
+    if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+    trace_mark(job.trace, tat, wi, 1);
+    // counters read after the barrier: the same values in every block, so the
+    // skips below are grid-uniform
+    const bool has_big = ld_cg_u32(&w.cnt->big_count) != 0;
+    const bool has_mut = ld_cg_u32(&w.cnt->mut_count) != 0;
+    if (has_big || split < w.n) {
+      if (has_big) phase_sort_big<Tr>(sc, w, smem);
+      if (split < w.n)  // small claims so blocks freed by the sort take more
+        phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
+                                  blockDim.x * P, job.dedup != 0, ProbeSel{split, w.n, false},
+                                  split & ~31u);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+    }
+    trace_mark(job.trace, tat, wi, 2);
+    if (has_mut) {
+      phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
+      phase_resolve_reads<Tr>(sc, w, tid, nt);
+    }
+    // Before the next window: its probes must see this window's writes, and
+    // its first thread resets this window's counter set, which every block
+    // must have finished reading.  The last window needs none (kernel end).
+    if (wi + 1 < nwin && !grid_barrier(bar, nblocks, t.status, seq)) return;
+    trace_mark(job.trace, tat, wi, 3);
   }
 }
 
@@ -157,6 +182,20 @@ __global__ void k_dump(TableView t, uint32_t buckets, typename Tr::Key* keys, ui
 }
 
 // ------------------------------------------------------------- tables
+struct Tuning {
+  uint32_t block = 512;  // threads per block (128..1024)
+  uint32_t chunk = 0;    // probe work claim (0 = static stride)
+  uint32_t prefetch = 1; // extra lookups in flight per thread (0..2)
+  uint32_t dedup = 1;
+};
+
+inline bool tuning_ok(const lsb_tuning& x) {
+  return (x.block_threads == 128 || x.block_threads == 256 || x.block_threads == 512 ||
+          x.block_threads == 1024) &&
+         x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
+         x.fused_split <= 100;
+}
+
 template <class Tr>
 struct Table {
   int device = 0;
@@ -173,9 +212,10 @@ struct Table {
   uint32_t epoch = 0;  // last epoch handed to a window
   uint32_t chunk = 1;  // per-SM pool refill size
   int num_sms = 0;
-  int plain_grid = 0;
-  int fused_grid = 0;
-  bool dedup = true;
+  Tuning tune;
+  uint32_t split_q16 = 65536;  // all of a window's reads probed before the sort pass
+  uint64_t* trace = nullptr;   // device phase-trace buffer when tracing is on
+  int fused_per_sm[3][4] = {};  // occupancy by (prefetch, block size) once queried
 
   TableView view() const {
     TableView v;
@@ -190,26 +230,16 @@ struct Table {
   }
 
   void release() {
-    cudaFree(slabs);
-    cudaFree(locks);
-    cudaFree(status);
-    cudaFree(pool);
-    cudaFree(bar);
-    cudaFree(sc.gtab);
-    cudaFree(sc.minfo);
-    cudaFree(sc.pred);
-    cudaFree(sc.goff);
-    cudaFree(sc.seg);
-    cudaFree(sc.sseg);
-    cudaFree(sc.mlist);
-    cudaFree(sc.big);
-    cudaFree(sc.cnt);
+    void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
+                    sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
+                    sc.cnt, trace};
+    for (void* p : ptrs) cudaFree(p);
   }
 
   int init(unsigned log2_buckets, const lsb_options* opt) {
     if (log2_buckets < 1 || log2_buckets > 30) return LSB_ERR_ARG;
     uint32_t window = opt && opt->max_window ? opt->max_window : kDefaultWindow;
-    if (window > kMaxWindow) return LSB_ERR_ARG;
+    if (window > kMaxWindow || window < 32) return LSB_ERR_ARG;
     if (opt && opt->lock_mode > kLockRW) return LSB_ERR_ARG;
     if (opt && opt->device >= 0) LSB_CK(cudaSetDevice(opt->device));
     LSB_CK(cudaGetDevice(&device));
@@ -223,26 +253,33 @@ struct Table {
                                          std::max<uint64_t>(1, pool_slabs / (8ull * num_sms)));
 
     const size_t slab_bytes = ((size_t)buckets + pool_slabs) * Tr::kSlabBytes;
-    uint32_t g = 2;
+    uint32_t g = 64;
     while (g < 2 * window) g <<= 1;
+    uint32_t cg = 64;  // chunk slots: at most window/kChunk full chunks + one per big group
+    while (cg < 2 * (window / kChunk + window / (kInline + 1) + 1)) cg <<= 1;
     sc.gmask = g - 1;
+    sc.cmask = cg - 1;
     sc.max_window = window;
-    if (cudaMalloc(&slabs, slab_bytes) != cudaSuccess ||
-        cudaMalloc(&locks, sizeof(int32_t) * buckets) != cudaSuccess ||
-        cudaMalloc(&status, sizeof(uint32_t)) != cudaSuccess ||
-        cudaMalloc(&pool, sizeof(uint64_t) * (2 + kPoolSlots)) != cudaSuccess ||
-        cudaMalloc(&bar, sizeof(GridBarrier)) != cudaSuccess ||
-        cudaMalloc(&sc.gtab, sizeof(uint64_t) * g) != cudaSuccess ||
-        cudaMalloc(&sc.minfo, sizeof(uint64_t) * window) != cudaSuccess ||
-        cudaMalloc(&sc.pred, sizeof(uint32_t) * window) != cudaSuccess ||
-        cudaMalloc(&sc.goff, sizeof(uint32_t) * g) != cudaSuccess ||
-        cudaMalloc(&sc.seg, sizeof(uint32_t) * window) != cudaSuccess ||
-        cudaMalloc(&sc.sseg, sizeof(uint32_t) * window) != cudaSuccess ||
-        cudaMalloc(&sc.mlist, sizeof(uint32_t) * window) != cudaSuccess ||
-        cudaMalloc(&sc.big, sizeof(uint32_t) * (window / kSmallGroup + 1)) != cudaSuccess ||
-        cudaMalloc(&sc.cnt, sizeof(WinCounters) * 2) != cudaSuccess) {
+    bool ok =
+        cudaMalloc(&slabs, slab_bytes) == cudaSuccess &&
+        cudaMalloc(&locks, sizeof(int32_t) * buckets) == cudaSuccess &&
+        cudaMalloc(&status, sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&pool, sizeof(uint64_t) * (2 + kPoolSlots)) == cudaSuccess &&
+        cudaMalloc(&sc.gtab, sizeof(uint64_t) * g) == cudaSuccess &&
+        cudaMalloc(&sc.ginl, sizeof(uint32_t) * kInline * (size_t)g) == cudaSuccess &&
+        cudaMalloc(&sc.ctab, sizeof(uint64_t) * cg) == cudaSuccess &&
+        cudaMalloc(&sc.cdat, sizeof(uint32_t) * kChunk * (size_t)cg) == cudaSuccess &&
+        cudaMalloc(&sc.minfo, sizeof(uint64_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.mloc, sizeof(uint64_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.pred, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.goff, sizeof(uint32_t) * g) == cudaSuccess &&
+        cudaMalloc(&sc.seg, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.mlist, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.big, sizeof(uint32_t) * (window / (kInline + 1) + 1)) == cudaSuccess &&
+        cudaMalloc(&sc.large, sizeof(uint32_t) * (window / (kWarpSort + 1) + 1)) == cudaSuccess &&
+        cudaMalloc(&sc.cnt, sizeof(WinCounters) * 2 + sizeof(GridBarrier)) == cudaSuccess;
+    if (!ok) {
       cudaGetLastError();
-      release();
       return LSB_ERR_OOM;
     }
     LSB_CK(cudaMemset(slabs, 0, slab_bytes));
@@ -252,27 +289,45 @@ struct Table {
     p[0] = buckets;
     p[1] = (uint64_t)buckets + pool_slabs;
     LSB_CK(cudaMemcpy(pool, p.data(), sizeof(uint64_t) * p.size(), cudaMemcpyHostToDevice));
-    LSB_CK(cudaMemset(bar, 0, sizeof(GridBarrier)));
     LSB_CK(cudaMemset(sc.gtab, 0, sizeof(uint64_t) * g));
-    LSB_CK(cudaMemset(sc.cnt, 0, sizeof(WinCounters) * 2));
-
-    plain_grid = num_sms * (2048 / kPlainBlock);
+    LSB_CK(cudaMemset(sc.ctab, 0, sizeof(uint64_t) * cg));
+    LSB_CK(cudaMemset(sc.cnt, 0, sizeof(WinCounters) * 2 + sizeof(GridBarrier)));
+    bar = reinterpret_cast<GridBarrier*>(sc.cnt + 2);
     LSB_CK(cudaFuncSetAttribute(k_sort<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
-    LSB_CK(cudaFuncSetAttribute(k_fused<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
-    int per_sm = 0;
-    LSB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<Tr>, kFusedBlock,
-                                                         kSortSmemBytes));
-    if (per_sm < 1) return LSB_ERR_STATE;
-    fused_grid = per_sm * num_sms;
+    LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSortSmemBytes));
+    LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSortSmemBytes));
     return LSB_OK;
   }
 
-  // Next epoch for a window; clears the group table when the 16-bit epoch wraps.
+  int set_tuning(const lsb_tuning& x) {
+    if (!tuning_ok(x)) return LSB_ERR_ARG;
+    tune.block = x.block_threads;
+    tune.chunk = x.chunk;
+    tune.prefetch = x.prefetch;
+    tune.dedup = x.dedup;
+    split_q16 = (uint32_t)(((uint64_t)x.fused_split << 16) / 100);
+    return LSB_OK;
+  }
+
+  void get_tuning(lsb_tuning* x) const {
+    x->block_threads = tune.block;
+    x->chunk = tune.chunk;
+    x->prefetch = tune.prefetch;
+    x->dedup = tune.dedup;
+    x->fused_split = (uint32_t)(((uint64_t)split_q16 * 100 + 32768) >> 16);
+  }
+
+  // Next epoch for a window; clears the group and chunk tables when the
+  // 16-bit epoch wraps.
   int next_epochs(uint32_t count, cudaStream_t s, uint32_t* first) {
     if (epoch + count > 0xFFFFu) {
       LSB_CK(cudaMemsetAsync(sc.gtab, 0, sizeof(uint64_t) * (sc.gmask + 1ull), s));
+      LSB_CK(cudaMemsetAsync(sc.ctab, 0, sizeof(uint64_t) * (sc.cmask + 1ull), s));
       epoch = 0;
     }
     *first = epoch + 1;
@@ -302,24 +357,39 @@ struct Table {
     return kind == kOutResult ? 16 : (kind == kOutOld ? 8 : 1);
   }
 
-  // Read-only batch: one probe launch, no scratch.
+  int grid_for(uint32_t n) const {
+    const int per_sm = 2048 / (int)tune.block;
+    const uint32_t need = (n + tune.block * (tune.prefetch + 1) - 1) / (tune.block * (tune.prefetch + 1));
+    return std::max(1, std::min<int>(per_sm * num_sms, (int)need));
+  }
+
+  template <bool kGroup>
+  void launch_probe(int grid, const Window<Tr>& w, cudaStream_t s) {
+    const TableView tv = view();
+    switch (tune.prefetch) {
+      case 0: k_probe<Tr, kGroup, 1><<<grid, tune.block, 0, s>>>(tv, sc, w, tune.chunk, tune.dedup); break;
+      case 1: k_probe<Tr, kGroup, 2><<<grid, tune.block, 0, s>>>(tv, sc, w, tune.chunk, tune.dedup); break;
+      default: k_probe<Tr, kGroup, 3><<<grid, tune.block, 0, s>>>(tv, sc, w, tune.chunk, tune.dedup); break;
+    }
+  }
+
+  // Read-only batch: one probe launch per 2^23 ops, no grouping.
   int run_reads(const typename Tr::Key* keys, void* out, uint32_t out_kind, size_t n,
                 cudaStream_t s) {
     for (size_t off = 0; off < n; off += (size_t)kMaxWindow) {
       uint32_t m = (uint32_t)std::min<size_t>(kMaxWindow, n - off);
       Window<Tr> w = window(nullptr, kOpRead, keys + off, 1, nullptr, 1,
                             out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr, out_kind, m);
-      int grid = std::min<int>(plain_grid, (int)((m + kPlainBlock - 1) / kPlainBlock));
-      if (dedup)
-        k_probe<Tr, false, true><<<grid, kPlainBlock, 0, s>>>(view(), sc, w);
-      else
-        k_probe<Tr, false, false><<<grid, kPlainBlock, 0, s>>>(view(), sc, w);
+      w.cnt = &sc.cnt[0];
+      if (tune.chunk) LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
+      launch_probe<false>(grid_for(m), w, s);
       LSB_CK(cudaGetLastError());
     }
     return LSB_OK;
   }
 
-  // General batch as per-phase launches, window by window.
+  // General batch as per-phase launches, window by window: probe, sort of
+  // big groups, resolve.
   int run_plain(const uint8_t* types, uint8_t uniform, const typename Tr::Key* keys,
                 uint32_t kstride, const uint64_t* vals, uint32_t vstride, void* out,
                 uint32_t out_kind, size_t n, cudaStream_t s) {
@@ -333,20 +403,28 @@ struct Table {
       if (e) return e;
       w.cnt = &sc.cnt[0];
       LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
-      int grid = std::min<int>(plain_grid, (int)((m + kPlainBlock - 1) / kPlainBlock));
-      grid = std::max(grid, 1);
-      TableView tv = view();
-      if (dedup)
-        k_probe<Tr, true, true><<<grid, kPlainBlock, 0, s>>>(tv, sc, w);
-      else
-        k_probe<Tr, true, false><<<grid, kPlainBlock, 0, s>>>(tv, sc, w);
-      k_segments<Tr><<<grid, kPlainBlock, 0, s>>>(sc, w);
-      k_scatter<Tr><<<grid, kPlainBlock, 0, s>>>(sc, w);
-      k_sort<Tr><<<std::max(grid, num_sms), kPlainBlock, kSortSmemBytes, s>>>(sc, w);
-      k_resolve<Tr><<<grid, kPlainBlock, 0, s>>>(tv, sc, w);
+      const int grid = grid_for(m);
+      launch_probe<true>(grid, w, s);
+      k_sort<Tr><<<num_sms, 256, kSortSmemBytes, s>>>(sc, w);
+      const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
+      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w);
       LSB_CK(cudaGetLastError());
     }
     return LSB_OK;
+  }
+
+  int fused_grid() {
+    const int pi = (int)tune.prefetch;
+    const int bi = tune.block == 128 ? 0 : tune.block == 256 ? 1 : tune.block == 512 ? 2 : 3;
+    int& per_sm = fused_per_sm[pi][bi];
+    if (per_sm == 0) {
+      const void* f = pi == 0 ? (const void*)k_fused<Tr, 1>
+                    : pi == 1 ? (const void*)k_fused<Tr, 2> : (const void*)k_fused<Tr, 3>;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, (int)tune.block,
+                                                        kSortSmemBytes) != cudaSuccess)
+        per_sm = -1;
+    }
+    return per_sm > 0 ? per_sm * num_sms : 0;
   }
 
   int run_fused(const uint8_t* types, uint8_t uniform, const typename Tr::Key* keys,
@@ -356,19 +434,26 @@ struct Table {
     FusedJob<Tr> job;
     job.base = window(types, uniform, keys, 1, vals, 1, out, out_kind, (uint32_t)n);
     job.window = sc.max_window;
+    job.chunk = tune.chunk;
+    job.dedup = tune.dedup;
+    job.split_q16 = split_q16;
+    job.trace = trace;
+    if (trace) LSB_CK(cudaMemsetAsync(trace, 0, sizeof(uint64_t) * kTraceCap, s));
     uint32_t nwin = (uint32_t)((n + job.window - 1) / job.window);
     if (nwin > 0xFFF0u) return LSB_ERR_ARG;
+    const int grid = fused_grid();
+    if (grid <= 0) return LSB_ERR_STATE;
     int e = next_epochs(nwin, s, &job.epoch0);
     if (e) return e;
-    LSB_CK(cudaMemsetAsync(sc.cnt, 0, sizeof(WinCounters) * 2, s));
-    LSB_CK(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s));
+    // counters of both windows and the barrier: one memset
+    LSB_CK(cudaMemsetAsync(sc.cnt, 0, sizeof(WinCounters) * 2 + sizeof(GridBarrier), s));
     TableView tv = view();
     Scratch scv = sc;
     GridBarrier* b = bar;
     void* args[] = {&tv, &scv, &job, &b};
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(fused_grid);
-    cfg.blockDim = dim3(kFusedBlock);
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(tune.block);
     cfg.dynamicSmemBytes = kSortSmemBytes;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -376,7 +461,32 @@ struct Table {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_fused<Tr>, args));
+    const void* f = tune.prefetch == 0 ? (const void*)k_fused<Tr, 1>
+                  : tune.prefetch == 1 ? (const void*)k_fused<Tr, 2> : (const void*)k_fused<Tr, 3>;
+    LSB_CK(cudaLaunchKernelExC(&cfg, f, args));
+    return LSB_OK;
+  }
+
+  int set_trace(int on) {
+    if (on && !trace) {
+      if (cudaMalloc(&trace, sizeof(uint64_t) * kTraceCap) != cudaSuccess) return LSB_ERR_OOM;
+      LSB_CK(cudaMemset(trace, 0, sizeof(uint64_t) * kTraceCap));
+    } else if (!on && trace) {
+      cudaFree(trace);
+      trace = nullptr;
+    }
+    return LSB_OK;
+  }
+
+  int read_trace(uint64_t* out, size_t cap, size_t* count, cudaStream_t s) {
+    if (!trace) return LSB_ERR_STATE;
+    std::vector<uint64_t> h(kTraceCap);
+    LSB_CK(cudaStreamSynchronize(s));
+    LSB_CK(cudaMemcpy(h.data(), trace, sizeof(uint64_t) * kTraceCap, cudaMemcpyDeviceToHost));
+    size_t n = 0;
+    while (n < kTraceCap && h[n] != 0) ++n;
+    for (size_t i = 0; i < n && i < cap; ++i) out[i] = h[i];
+    if (count) *count = n;
     return LSB_OK;
   }
 
@@ -544,6 +654,27 @@ int lsb_map_execute_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys
 
 uint32_t lsb_map_buckets(const lsb_map* m) { return m ? m->t.buckets : 0; }
 
+int lsb_map_get_tuning(const lsb_map* m, lsb_tuning* out) {
+  if (!m || !out) return LSB_ERR_ARG;
+  m->t.get_tuning(out);
+  return LSB_OK;
+}
+
+int lsb_map_set_tuning(lsb_map* m, const lsb_tuning* t) {
+  if (!m || !t) return LSB_ERR_ARG;
+  return m->t.set_tuning(*t);
+}
+
+int lsb_map_set_trace(lsb_map* m, int on) {
+  if (!m) return LSB_ERR_ARG;
+  return m->t.set_trace(on);
+}
+
+int lsb_map_read_trace(lsb_map* m, uint64_t* out, size_t cap, size_t* count, cudaStream_t s) {
+  if (!m || (cap && !out)) return LSB_ERR_ARG;
+  return m->t.read_trace(out, cap, count, s);
+}
+
 int lsb_map_status(lsb_map* m, uint32_t* flags, cudaStream_t s) {
   if (!m) return LSB_ERR_ARG;
   return m->t.read_status(flags, s);
@@ -632,6 +763,27 @@ int lsb_set_execute_fused(lsb_set* p, const uint8_t* types, const uint32_t* keys
 }
 
 uint32_t lsb_set_buckets(const lsb_set* p) { return p ? p->t.buckets : 0; }
+
+int lsb_set_get_tuning(const lsb_set* p, lsb_tuning* out) {
+  if (!p || !out) return LSB_ERR_ARG;
+  p->t.get_tuning(out);
+  return LSB_OK;
+}
+
+int lsb_set_set_tuning(lsb_set* p, const lsb_tuning* t) {
+  if (!p || !t) return LSB_ERR_ARG;
+  return p->t.set_tuning(*t);
+}
+
+int lsb_set_set_trace(lsb_set* p, int on) {
+  if (!p) return LSB_ERR_ARG;
+  return p->t.set_trace(on);
+}
+
+int lsb_set_read_trace(lsb_set* p, uint64_t* out, size_t cap, size_t* count, cudaStream_t s) {
+  if (!p || (cap && !out)) return LSB_ERR_ARG;
+  return p->t.read_trace(out, cap, count, s);
+}
 
 int lsb_set_status(lsb_set* p, uint32_t* flags, cudaStream_t s) {
   if (!p) return LSB_ERR_ARG;

@@ -93,6 +93,69 @@ __device__ __forceinline__ uint64_t ld_cg_u64(const void* p) {
   return r;
 }
 
+// L1-cached loads for the read-only probe.  Safe because no table write runs
+// concurrently with a probe (calls that mutate a table are stream-ordered;
+// inside the persistent kernel probes and writes are separated by grid
+// barriers whose acquire fence makes the SM's L1 observe earlier writes).
+// Hot Zipf keys then hit each SM's L1 instead of queueing at one L2 slice.
+// The loads also carry an L2 evict_last policy, and the streaming batch
+// inputs/outputs an evict_first one, so the table's hot sectors outlive the
+// batch data in L2 across calls.
+__device__ __forceinline__ uint64_t l2_keep() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint4 ld_ca_v4(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.ca.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p), "l"(l2_keep()));
+  return r;
+}
+
+__device__ __forceinline__ ulonglong2 ld_ca_v2u64(const void* p) {
+  ulonglong2 r;
+  asm volatile("ld.global.ca.L2::cache_hint.v2.u64 {%0,%1}, [%2], %3;"
+               : "=l"(r.x), "=l"(r.y)
+               : "l"(p), "l"(l2_keep()));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t ld_ca_u32(const void* p) {
+  uint32_t r;
+  asm volatile("ld.global.ca.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(l2_keep()));
+  return r;
+}
+
+// Streaming (read-once / write-once) batch data: evict-first in L1 and L2.
+__device__ __forceinline__ uint64_t ld_cs_u64(const void* p) {
+  uint64_t r;
+  asm volatile("ld.global.cs.u64 %0, [%1];" : "=l"(r) : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ uint32_t ld_cs_u32(const void* p) {
+  uint32_t r;
+  asm volatile("ld.global.cs.u32 %0, [%1];" : "=r"(r) : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ uint8_t ld_cs_u8(const void* p) {
+  unsigned short r;
+  asm volatile("ld.global.cs.u8 %0, [%1];" : "=h"(r) : "l"(p));
+  return (uint8_t)r;
+}
+
+__device__ __forceinline__ void st_cs_u64(void* p, uint64_t v) {
+  asm volatile("st.global.cs.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_cs_u8(void* p, uint8_t v) {
+  asm volatile("st.global.cs.u8 [%0], %1;" ::"l"(p), "h"((unsigned short)v) : "memory");
+}
+
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
   uint32_t r;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
@@ -135,9 +198,10 @@ struct Meta {
   uint32_t tag[7];  // 28 tag bytes, slot s in byte (s & 3) of word s >> 2
 };
 
+template <bool kL1 = false>
 __device__ __forceinline__ Meta load_meta(const uint8_t* slab) {
-  uint4 a = ld_cg_v4(slab);
-  uint4 b = ld_cg_v4(slab + 16);
+  uint4 a = kL1 ? ld_ca_v4(slab) : ld_cg_v4(slab);
+  uint4 b = kL1 ? ld_ca_v4(slab + 16) : ld_cg_v4(slab + 16);
   Meta m;
   m.next = a.x;
   m.tag[0] = a.y; m.tag[1] = a.z; m.tag[2] = a.w;
@@ -277,35 +341,106 @@ __device__ __forceinline__ void unlock_reader(const TableView& t, uint32_t bucke
 
 // ---------------------------------------------------------------- probe
 // Thread-per-op lookup: per slab one 32-B meta sector, then one slot load per
-// fingerprint candidate.  Returns 1 if found (value in *val for the map).
+// fingerprint candidate.  A hit also reports where the key lives, packed as
+// kLocLive | slab << 8 | slot, so the op's later write can go straight there.
+constexpr uint64_t kLocLive = 1ull << 63;
+
+__device__ __forceinline__ uint32_t loc_slab(uint64_t loc) { return (uint32_t)(loc >> 8); }
+__device__ __forceinline__ int loc_slot(uint64_t loc) { return (int)(loc & 0xFFu); }
+
+// Continue a lookup in slab `s` whose meta is `m`, trying candidate slots
+// `cand`, then the rest of the chain.
 template <class Tr>
-__device__ __forceinline__ bool table_find(const TableView& t, typename Tr::Key key, uint64_t h,
-                                           uint64_t* val) {
-  uint32_t s = (uint32_t)h & t.mask;
-  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
+__device__ __noinline__ bool find_rest(const TableView& t, typename Tr::Key key, uint32_t rep,
+                                       uint32_t s, Meta m, uint32_t cand, uint64_t* val,
+                                       uint64_t* loc) {
   for (uint32_t hop = 0; hop < kMaxHops; ++hop) {
     const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
-    Meta m = load_meta(slab);
-    uint32_t cand = tag_match(m, rep);
     while (cand) {
       int slot = __ffs(cand) - 1;
       cand &= cand - 1;
       if constexpr (Tr::kHasValue) {
-        ulonglong2 kv = ld_cg_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
+        ulonglong2 kv = ld_ca_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
         if (kv.x == (uint64_t)key) {
           *val = kv.y;
+          *loc = kLocLive | ((uint64_t)s << 8) | (uint64_t)slot;
           return true;
         }
       } else {
-        uint32_t k = ld_cg_u32(slab + kMetaBytes + slot * Tr::kSlotBytes);
-        if (k == (uint32_t)key) return true;
+        if (ld_ca_u32(slab + kMetaBytes + slot * Tr::kSlotBytes) == (uint32_t)key) {
+          *loc = kLocLive | ((uint64_t)s << 8) | (uint64_t)slot;
+          return true;
+        }
       }
     }
     s = m.next;
     if (s == 0) return false;
+    m = load_meta<true>(slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes));
+    cand = tag_match(m, rep);
   }
   raise_status(t.status, kStatusChain);
   return false;
+}
+
+template <class Tr>
+__device__ __forceinline__ bool table_find(const TableView& t, typename Tr::Key key, uint64_t h,
+                                           uint64_t* val, uint64_t* loc) {
+  const uint32_t s = (uint32_t)h & t.mask;
+  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
+  Meta m = load_meta<true>(slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes));
+  return find_rest<Tr>(t, key, rep, s, m, tag_match(m, rep), val, loc);
+}
+
+// P independent lookups issued together: all head meta sectors first, then
+// all first-candidate slots, so a thread keeps up to P loads in flight.  The
+// rare rest (second candidate, longer chain) falls back to find_rest.
+template <class Tr, int P>
+__device__ __forceinline__ void table_find_n(const TableView& t, const typename Tr::Key* key,
+                                             const uint64_t* h, const bool* want, bool* found,
+                                             uint64_t* val, uint64_t* loc) {
+  Meta m[P];
+  uint32_t rep[P], s[P], cand[P];
+  const uint8_t* base = (const uint8_t*)t.slabs;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    s[j] = (uint32_t)h[j] & t.mask;
+    rep[j] = (0x80u | fingerprint(h[j])) * 0x01010101u;
+    if (want[j]) m[j] = load_meta<true>(slab_ptr(base, s[j], Tr::kSlabBytes));
+  }
+  uint64_t k0[P], v0[P];
+  int slot0[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    cand[j] = want[j] ? tag_match(m[j], rep[j]) : 0u;
+    slot0[j] = cand[j] ? __ffs(cand[j]) - 1 : -1;
+    if (slot0[j] >= 0) {
+      const uint8_t* sp = slab_ptr(base, s[j], Tr::kSlabBytes) + kMetaBytes + slot0[j] * Tr::kSlotBytes;
+      if constexpr (Tr::kHasValue) {
+        ulonglong2 kv = ld_ca_v2u64(sp);
+        k0[j] = kv.x;
+        v0[j] = kv.y;
+      } else {
+        k0[j] = ld_ca_u32(sp);
+        v0[j] = 0;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    found[j] = false;
+    val[j] = 0;
+    loc[j] = 0;
+    if (!want[j]) continue;
+    if (slot0[j] >= 0 && k0[j] == (uint64_t)key[j]) {
+      found[j] = true;
+      val[j] = v0[j];
+      loc[j] = kLocLive | ((uint64_t)s[j] << 8) | (uint64_t)slot0[j];
+    } else if (cand[j] & (cand[j] - 1) || m[j].next != 0) {
+      found[j] = find_rest<Tr>(t, key[j], rep[j], s[j], m[j],
+                               slot0[j] >= 0 ? cand[j] & (cand[j] - 1) : cand[j], &val[j],
+                               &loc[j]);
+    }
+  }
 }
 
 // ---------------------------------------------------------------- apply
@@ -516,38 +651,69 @@ __device__ __forceinline__ void table_apply(const TableView& t, typename Tr::Key
     table_apply_locked<Tr>(t, key, h, present, val);
 }
 
+// Write the final state of a key whose live slot is known from this window's
+// probe (loc has kLocLive).  Only this thread writes that key, and a live
+// slot keeps its key until its own key's writer tombstones it, so neither a
+// lock nor a rescan is needed: an update is one value store, a removal clears
+// the live bit of the tag with an atomic (other bytes of the word may be
+// changing under other writers).  Absent keys take table_apply.
+template <class Tr>
+__device__ __forceinline__ void table_apply_known(const TableView& t, typename Tr::Key key,
+                                                  uint64_t h, uint64_t loc, bool present,
+                                                  uint64_t val) {
+  if (!(loc & kLocLive)) {
+    if (present) table_apply<Tr>(t, key, h, true, val);
+    return;
+  }
+  uint8_t* slab = slab_ptr(t.slabs, loc_slab(loc), Tr::kSlabBytes);
+  const int slot = loc_slot(loc);
+  if (present) {
+    if constexpr (Tr::kHasValue) st_cg_u64(slab + kMetaBytes + slot * Tr::kSlotBytes + 8, val);
+  } else {
+    // An atomic on the tag word: a locked insert of another key may be
+    // writing a neighbouring tag byte of the same word at the same time.
+    atomicAnd(tag_word(slab, slot), ~(0x80u << (8 * (slot & 3))));
+  }
+}
+
 // -------------------------------------------------------- grid barrier
-// Sense-counting barrier for a cooperative (co-resident) grid.  Each wait
-// polls at most kBarrierPolls times; on timeout it raises kStatusBarrier and
-// returns false so the caller can leave the kernel.
+// Monotonic-count barrier for a cooperative (co-resident) grid: barrier k of
+// a launch completes when the arrival counter reaches (k + 1) * nblocks, so
+// nothing is reset between barriers.  One thread per block arrives with a
+// release add and polls with acquire loads; the block's other threads are
+// ordered by __syncthreads on both sides.  Each wait polls at most
+// kBarrierPolls times; on timeout it raises kStatusBarrier and returns false
+// so the caller can leave the kernel.
 struct GridBarrier {
-  uint32_t count;
-  uint32_t gen;
+  uint32_t count;  // arrivals in this launch (zeroed before the launch)
+  uint32_t pad;
 };
 
-__device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status) {
-  __syncthreads();
+__device__ __forceinline__ uint32_t atom_add_release(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status,
+                                             uint32_t& seq) {
   __shared__ int ok;
+  __syncthreads();
+  ++seq;
   if (threadIdx.x == 0) {
     ok = 1;
-    uint32_t g = ld_acquire_u32(&b->gen);
-    __threadfence();
-    if (atomicAdd(&b->count, 1u) == nblocks - 1) {
-      b->count = 0;
-      __threadfence();
-      st_release_u32(&b->gen, g + 1);
-    } else {
+    const uint32_t target = seq * nblocks;
+    if (atom_add_release(&b->count, 1u) + 1 != target) {
       uint32_t it = 0;
-      while (ld_acquire_u32(&b->gen) == g) {
+      while ((int32_t)(ld_acquire_u32(&b->count) - target) < 0) {
         if (++it > kBarrierPolls || (*(volatile uint32_t*)status & kStatusBarrier)) {
           raise_status(status, kStatusBarrier);
           ok = 0;
           break;
         }
-        __nanosleep(it < 64 ? 20 : 200);
+        if (it > 256) __nanosleep(64);
       }
     }
-    __threadfence();
   }
   __syncthreads();
   return ok != 0;

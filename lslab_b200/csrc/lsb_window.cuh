@@ -2,44 +2,48 @@
 // key repetition) with results equal to running them one at a time in index
 // order.
 //
-// Phases of one window (each a grid-stride pass; a grid-wide barrier or a
-// kernel boundary between them):
-//   A probe     every op reads the table (pre-window state) and writes that
-//               as its tentative result; mutations join a per-key group in a
-//               scratch hash table (open addressing, epoch-tagged slots so
-//               nothing is cleared between windows) and list themselves.
-//   B segment   each group with more than one mutation reserves a segment.
-//   C scatter   mutations write their op index into their group's segment.
-//   D sort      segments are sorted by op index (one thread for <= 16
-//               entries, a block-wide bitmap counting sort above), and each
-//               mutation learns its predecessor in index order and whether
-//               it is the group's last.
-//   E resolve   a mutation with a predecessor takes its result from it (the
-//               predecessor's post-state: put -> {1, value}, remove -> {0, 0});
-//               each group's last mutation writes the final state to the
-//               table; a read after the window's first mutation looks its key
-//               up among the groups and, if some mutation of that key precedes
-//               it, takes its result from the latest one (binary search of the
-//               sorted segment).
-// Only phase E writes the table, and only one thread per key does, so no
-// read ever races a same-key write; reads of other keys in the same bucket
-// stay correct because the apply publishes slots with a fence before the tag.
+// Phases of one window (grid-stride passes; a grid-wide barrier or a kernel
+// boundary between them):
+//   A probe    every op reads the table (pre-window state, P lookups in flight
+//              per thread) and writes that as its tentative result.  Each
+//              mutation joins its key's group in a scratch hash table
+//              (epoch-tagged slots, never cleared) and gets a position in it;
+//              positions 0..7 are stored inline in the group, later ones in
+//              32-entry chunks found through a second small hash table.  The
+//              mutation also records where its key lives (the probe's slot).
+//   D sort     only groups with more than 8 mutations: one block gathers the
+//              group, orders it by op index, stores the sorted list and every
+//              member's predecessor.  Skipped when no such group exists.
+//   E resolve  a mutation takes its result from its predecessor in index
+//              order (that op's post-state: put -> {1, value}, remove ->
+//              {0, 0}); the group's last mutation writes the final state (a
+//              value store or tag flip at the recorded slot, or a locked
+//              insert for a key that was absent).  A read after the window's
+//              first mutation finds its key's group and, if a mutation of that
+//              key precedes it, takes that mutation's post-state.
+// Only phase E writes the table and only one thread per key does, so no probe
+// races a same-key write.
 //
 // The reference runs each op under a per-bucket warp lock in lane order within
 // a warp and in lock-acquisition order across warps
-// (include/lslab/detail/traverse.h:39-143); the engine replaces that with an
-// order fixed by op index, computed without locks on the read path.
+// (include/lslab/detail/traverse.h:39-143); the engine fixes the order by op
+// index instead and keeps locks off the read path.
 #pragma once
 
 #include "lsb_core.cuh"
 
 namespace lsb {
 
-constexpr uint32_t kSmallGroup = 16;
+constexpr uint32_t kInline = 8;        // group members stored inline
+constexpr uint32_t kChunk = 32;        // members per overflow chunk
 constexpr uint32_t kPredLast = 0x80000000u;
 constexpr uint32_t kPredMask = 0x7FFFFFFFu;  // predecessor op index + 1; 0 = none
-constexpr uint32_t kSortChunkWords = 4096;  // bitmap words per counting-sort chunk
-constexpr uint32_t kSortSmemBytes = 2 * kSortChunkWords * 4;
+constexpr uint32_t kWarpSort = 64;    // groups up to this size are ordered by one warp
+constexpr uint32_t kSortSmall = 4096;  // larger groups up to this size sort in shared memory
+constexpr uint32_t kSortChunkWords = 2048;  // bitmap words per counting-sort pass
+// shared memory of the sort: kSortSmall members + kSortSmall sorted + bitmap
+// + prefix words
+constexpr uint32_t kSortSmemBytes = (2 * kSortSmall + 2 * kSortChunkWords) * 4;
 
 // Group-table slot: bits 0..23 owner (op index + 1), 24..47 count, 48..63 epoch.
 __device__ __forceinline__ uint32_t g_owner(uint64_t v) { return (uint32_t)(v & 0xFFFFFFu); }
@@ -53,6 +57,10 @@ struct WinCounters {
   uint32_t big_count;
   uint32_t big_work;
   uint32_t inv_first_mut;  // ~(lowest mutation index); 0 = no mutation
+  uint32_t probe_cursor;   // next op to hand out when the probe claims chunks
+  uint32_t large_count;    // groups with more than kWarpSort members
+  uint32_t large_work;
+  uint32_t late_cursor;    // next late read handed out in the fused sort pass
   uint32_t pad[3];
 };
 
@@ -62,20 +70,30 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->big_count = 0;
   c->big_work = 0;
   c->inv_first_mut = 0;
+  c->probe_cursor = 0;
+  c->large_count = 0;
+  c->large_work = 0;
+  c->late_cursor = 0;
 }
 
 // Scratch owned by a table, sized for max_window ops.
 struct Scratch {
   uint64_t* gtab;   // group table, gmask + 1 slots
+  uint32_t* ginl;   // kInline members per group slot
+  uint64_t* ctab;   // overflow chunk table: epoch:16 | group slot:24 | chunk:24
+  uint32_t* cdat;   // kChunk members per chunk slot
   uint32_t gmask;
+  uint32_t cmask;
   uint32_t max_window;
-  uint64_t* minfo;  // per op: group slot << 32 | position in group
-  uint32_t* pred;   // per op: predecessor + 1 | kPredLast
-  uint32_t* goff;   // per group slot: segment offset
-  uint32_t* seg;    // unsorted segments
-  uint32_t* sseg;   // sorted segments
+  uint32_t pad;
+  uint64_t* minfo;  // per mutation: group slot << 32 | position in group
+  uint64_t* mloc;   // per mutation: the key's slot from the probe (0 = absent)
+  uint32_t* pred;   // per member of a big group: predecessor + 1 | kPredLast
+  uint32_t* goff;   // per big group slot: offset of its sorted list in seg
+  uint32_t* seg;    // sorted member lists of big groups
   uint32_t* mlist;  // mutation op indices
-  uint32_t* big;    // group slots with more than kSmallGroup mutations
+  uint32_t* big;    // group slots with more than kInline members
+  uint32_t* large;  // group slots with more than kWarpSort members
   WinCounters* cnt; // two sets, used by alternate windows
 };
 
@@ -90,7 +108,7 @@ struct Window {
   uint32_t kstride;      // elements between consecutive keys (2 for AoS pairs)
   uint32_t vstride;      // elements between consecutive values
   uint32_t n;
-  uint32_t epoch;  // 1..65535
+  uint32_t epoch;        // 1..65535
   uint8_t uniform;
   uint8_t out_kind;
   WinCounters* cnt;
@@ -111,6 +129,20 @@ __device__ __forceinline__ uint64_t val_of(const Window<Tr>& w, uint32_t i) {
   return w.vals[(size_t)i * w.vstride];
 }
 
+// First (streaming) read of op i's type and key in the probe phase.
+template <class Tr>
+__device__ __forceinline__ uint8_t op_type_stream(const Window<Tr>& w, uint32_t i) {
+  return w.types ? ld_cs_u8(w.types + i) : w.uniform;
+}
+
+template <class Tr>
+__device__ __forceinline__ typename Tr::Key key_stream(const Window<Tr>& w, uint32_t i) {
+  if constexpr (sizeof(typename Tr::Key) == 8)
+    return (typename Tr::Key)ld_cs_u64(w.keys + (size_t)i * w.kstride);
+  else
+    return (typename Tr::Key)ld_cs_u32(w.keys + (size_t)i * w.kstride);
+}
+
 // Result of op i given the key's state just before it.
 template <class Tr>
 __device__ __forceinline__ void write_result(const Window<Tr>& w, uint32_t i, uint8_t type,
@@ -119,15 +151,15 @@ __device__ __forceinline__ void write_result(const Window<Tr>& w, uint32_t i, ui
     case kOutResult: {
       // two 8-byte stores: lsb_result arrays are only 8-byte aligned in C
       uint64_t* p = (uint64_t*)w.out + 2 * (size_t)i;
-      st_cg_u64(p, found ? 1ull : 0ull);
-      st_cg_u64(p + 1, found ? value : 0ull);
+      st_cs_u64(p, found ? 1ull : 0ull);
+      st_cs_u64(p + 1, found ? value : 0ull);
       break;
     }
     case kOutOld:
-      ((uint64_t*)w.out)[i] = found ? value : 0ull;
+      st_cs_u64((uint64_t*)w.out + i, found ? value : 0ull);
       break;
     case kOutBool:
-      ((uint8_t*)w.out)[i] = (type == kOpWrite) ? 1 : (found ? 1 : 0);
+      st_cs_u8((uint8_t*)w.out + i, (type == kOpWrite) ? 1 : (found ? 1 : 0));
       break;
     default:
       break;
@@ -140,82 +172,175 @@ __device__ __forceinline__ uint32_t lane_id() {
   return l;
 }
 
-// ---------------------------------------------------------------- phase A
-// Returns the op's group slot and position through minfo; mutation indices
-// are appended to mlist (warp-aggregated).
-template <class Tr>
-__device__ __forceinline__ void group_join(const Scratch& sc, const Window<Tr>& w, uint32_t i,
-                                           typename Tr::Key key, uint64_t h) {
-  uint32_t slot = (uint32_t)(h >> 20) & sc.gmask;
-  const uint64_t mine = ((uint64_t)w.epoch << 48) | (1ull << 24) | (uint64_t)(i + 1);
-  for (uint32_t probe = 0; probe <= sc.gmask; ++probe) {
-    uint64_t v = ld_relaxed_u64(&sc.gtab[slot]);
-    if (g_epoch(v) != w.epoch) {
-      uint64_t prev = atomicCAS((unsigned long long*)&sc.gtab[slot], v, mine);
-      if (prev == v) {
-        sc.minfo[i] = ((uint64_t)slot << 32);
-        return;
-      }
+__device__ __forceinline__ uint32_t gslot_of(uint64_t h, uint32_t gmask) {
+  return (uint32_t)(h >> 20) & gmask;
+}
+
+// --------------------------------------------------------- overflow chunks
+__device__ __forceinline__ uint32_t chunk_hash(uint32_t gslot, uint32_t k) {
+  uint32_t x = gslot * 0x9E3779B1u ^ (k + 0x7F4A7C15u) * 0x85EBCA77u;
+  x ^= x >> 15;
+  x *= 0x2C1B3C6Du;
+  return x ^ (x >> 12);
+}
+
+// Slot of chunk k of group gslot in this window; claims it if new.
+__device__ __forceinline__ uint32_t chunk_claim(const Scratch& sc, uint32_t epoch, uint32_t gslot,
+                                                uint32_t k) {
+  const uint64_t key = ((uint64_t)epoch << 48) | ((uint64_t)gslot << 24) | k;
+  uint32_t s = chunk_hash(gslot, k) & sc.cmask;
+  for (uint32_t probe = 0; probe <= sc.cmask; ++probe) {
+    uint64_t v = ld_relaxed_u64(&sc.ctab[s]);
+    while ((uint32_t)(v >> 48) != epoch) {  // stale: try to claim
+      uint64_t prev = atomicCAS((unsigned long long*)&sc.ctab[s], v, key);
+      if (prev == v) return s;
       v = prev;
-      if (g_epoch(v) != w.epoch) {  // changed but still stale: retry this slot
-        --probe;
-        continue;
-      }
     }
-    if (key_of(w, g_owner(v) - 1) == key) {
-      uint64_t old = atomicAdd((unsigned long long*)&sc.gtab[slot], 1ull << 24);
-      sc.minfo[i] = ((uint64_t)slot << 32) | g_count(old);
-      return;
-    }
-    slot = (slot + 1) & sc.gmask;
+    if (v == key) return s;
+    s = (s + 1) & sc.cmask;
+  }
+  return 0xFFFFFFFFu;
+}
+
+__device__ __forceinline__ uint32_t chunk_find(const Scratch& sc, uint32_t epoch, uint32_t gslot,
+                                               uint32_t k) {
+  const uint64_t key = ((uint64_t)epoch << 48) | ((uint64_t)gslot << 24) | k;
+  uint32_t s = chunk_hash(gslot, k) & sc.cmask;
+  for (uint32_t probe = 0; probe <= sc.cmask; ++probe) {
+    uint64_t v = ld_relaxed_u64(&sc.ctab[s]);
+    if (v == key) return s;
+    if ((uint32_t)(v >> 48) != epoch) return 0xFFFFFFFFu;
+    s = (s + 1) & sc.cmask;
+  }
+  return 0xFFFFFFFFu;
+}
+
+// Member j (0-based position) of group gslot.
+__device__ __forceinline__ uint32_t member_at(const Scratch& sc, uint32_t epoch, uint32_t gslot,
+                                              uint32_t j) {
+  if (j < kInline) return ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + j]);
+  const uint32_t q = j - kInline;
+  const uint32_t cs = chunk_find(sc, epoch, gslot, q / kChunk);
+  return cs == 0xFFFFFFFFu ? 0xFFFFFFFFu : ld_cg_u32(&sc.cdat[(size_t)cs * kChunk + q % kChunk]);
+}
+
+// ---------------------------------------------------------------- phase A
+// Store member i at position pos of group `slot` (inline or in a chunk).
+template <class Tr>
+__device__ __forceinline__ void group_store(const Scratch& sc, const Window<Tr>& w, uint32_t slot,
+                                            uint32_t pos, uint32_t i, uint64_t loc) {
+  sc.minfo[i] = ((uint64_t)slot << 32) | pos;
+  sc.mloc[i] = loc;
+  if (pos >= sc.max_window) return;  // no group (cannot happen: the table has 2x room)
+  if (pos < kInline) {
+    sc.ginl[(size_t)slot * kInline + pos] = i;
+  } else {
+    const uint32_t q = pos - kInline;
+    const uint32_t cs = chunk_claim(sc, w.epoch, slot, q / kChunk);
+    if (cs != 0xFFFFFFFFu) sc.cdat[(size_t)cs * kChunk + q % kChunk] = i;
+    if (pos == kInline) sc.big[atomicAdd(&w.cnt->big_count, 1u)] = slot;
+    if (pos == kWarpSort) sc.large[atomicAdd(&w.cnt->large_count, 1u)] = slot;
   }
 }
 
-// Phase A over ops [begin, end) with a warp-uniform grid stride.  kGroup:
-// mutations join groups (false for read-only batches).  kDedup: lanes of a
-// warp that carry the same key share one probe.
-template <class Tr, bool kGroup, bool kDedup>
-__device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<Tr>& w,
-                            uint32_t warp_id, uint32_t num_warps) {
-  const uint32_t lane = lane_id();
-  const uint32_t lanemask_lt = (1u << lane) - 1u;
-  for (uint32_t base = warp_id * 32; base < w.n; base += num_warps * 32) {
-    const uint32_t i = base + lane;
-    const bool active = i < w.n;
-    const uint8_t type = active ? op_type(w, i) : kOpRead;
-    const typename Tr::Key key = active ? key_of(w, i) : (typename Tr::Key)0;
-    const uint64_t h = Tr::hash(key);
-    bool found = false;
-    uint64_t value = 0;
-    bool leader = active;
-    uint32_t src = lane;
-    if (kDedup) {
-      const uint32_t am = __ballot_sync(0xFFFFFFFFu, active);
-      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key) & am;
-      src = active ? (uint32_t)(__ffs(peers) - 1) : lane;
-      leader = active && src == lane;
+// Join `cnt` mutations of `key` (op indices carried by the caller's peer
+// lanes) to the key's group; returns the group slot and the position of the
+// first of them.  The group's owner (first joiner) claims the slot by CAS.
+template <class Tr>
+__device__ __forceinline__ uint32_t group_join(const Scratch& sc, const Window<Tr>& w, uint32_t i,
+                                               typename Tr::Key key, uint64_t h, uint32_t cnt,
+                                               uint32_t* pos_out) {
+  uint32_t slot = gslot_of(h, sc.gmask);
+  const uint64_t mine =
+      ((uint64_t)w.epoch << 48) | ((uint64_t)cnt << 24) | (uint64_t)(i + 1);
+  for (uint32_t probe = 0; probe <= sc.gmask; ++probe) {
+    uint64_t v = ld_relaxed_u64(&sc.gtab[slot]);
+    while (g_epoch(v) != w.epoch) {  // stale slot: try to claim it
+      uint64_t prev = atomicCAS((unsigned long long*)&sc.gtab[slot], v, mine);
+      if (prev == v) {
+        *pos_out = 0;
+        return slot;
+      }
+      v = prev;
     }
-    if (leader) {
-      const uint32_t bucket = (uint32_t)h & t.mask;
-      if (t.lock_mode == kLockRW) {
-        if (lock_reader(t, bucket)) {
-          found = table_find<Tr>(t, key, h, &value);
-          unlock_reader(t, bucket);
-        }
-      } else {
-        found = table_find<Tr>(t, key, h, &value);
+    if (key_of(w, g_owner(v) - 1) == key) {
+      *pos_out = g_count(atomicAdd((unsigned long long*)&sc.gtab[slot], (uint64_t)cnt << 24));
+      return slot;
+    }
+    slot = (slot + 1) & sc.gmask;
+  }
+  *pos_out = 0xFFFFFFFFu;
+  return 0;
+}
+
+// One tile of phase A: ops base + j*32 + lane for j < P.  kGroup: mutations
+// join groups (false for read-only batches).  dedup: lanes of a warp that
+// carry the same key share one lookup (warp-uniform flag).
+// Which ops a probe pass handles: reads with read_lo <= i < read_hi, and the
+// mutations when `muts` is set (the fused kernel splits a window's reads
+// between the grouping pass and the sort pass to hide the latter).
+struct ProbeSel {
+  uint32_t read_lo, read_hi;
+  bool muts;
+};
+
+template <class Tr, bool kGroup, int P>
+__device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc,
+                                           const Window<Tr>& w, uint32_t base, uint32_t lane,
+                                           bool dedup, const ProbeSel& sel) {
+  using Key = typename Tr::Key;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  Key key[P];
+  uint64_t h[P], value[P], loc[P];
+  uint8_t type[P];
+  bool active[P], want[P], found[P];
+  uint32_t src[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const uint32_t i = base + j * 32 + lane;
+    type[j] = i < w.n ? op_type_stream(w, i) : kOpRead;
+    active[j] = i < w.n && (type[j] == kOpRead ? (i >= sel.read_lo && i < sel.read_hi) : sel.muts);
+    key[j] = active[j] ? key_stream(w, i) : (Key)0;
+    h[j] = Tr::hash(key[j]);
+    want[j] = active[j];
+    src[j] = lane;
+    if (dedup) {
+      const uint32_t am = __ballot_sync(0xFFFFFFFFu, active[j]);
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[j]) & am;
+      if (active[j]) src[j] = __ffs(peers) - 1;
+      want[j] = active[j] && src[j] == lane;
+    }
+  }
+  if (t.lock_mode == kLockRW) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      found[j] = false;
+      value[j] = 0;
+      loc[j] = 0;
+      if (!want[j]) continue;
+      const uint32_t bucket = (uint32_t)h[j] & t.mask;
+      if (lock_reader(t, bucket)) {
+        found[j] = table_find<Tr>(t, key[j], h[j], &value[j], &loc[j]);
+        unlock_reader(t, bucket);
       }
     }
-    if (kDedup) {
-      found = __shfl_sync(0xFFFFFFFFu, found, src);
-      value = __shfl_sync(0xFFFFFFFFu, value, src);
+  } else {
+    table_find_n<Tr, P>(t, key, h, want, found, value, loc);
+  }
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    if (dedup) {
+      found[j] = __shfl_sync(0xFFFFFFFFu, found[j], src[j]);
+      value[j] = __shfl_sync(0xFFFFFFFFu, value[j], src[j]);
+      loc[j] = __shfl_sync(0xFFFFFFFFu, loc[j], src[j]);
     }
-    if (active) write_result(w, i, type, found, value);
+    const uint32_t i = base + j * 32 + lane;
+    if (active[j]) write_result(w, i, type[j], found[j], value[j]);
     if (kGroup) {
-      const bool is_mut = active && type != kOpRead;
+      const bool is_mut = active[j] && type[j] != kOpRead;
       const uint32_t mm = __ballot_sync(0xFFFFFFFFu, is_mut);
       if (mm) {
-        uint32_t first = __reduce_min_sync(0xFFFFFFFFu, is_mut ? i : 0xFFFFFFFFu);
+        const uint32_t first = __reduce_min_sync(0xFFFFFFFFu, is_mut ? i : 0xFFFFFFFFu);
         uint32_t slot_base = 0;
         const uint32_t ldr = __ffs(mm) - 1;
         if (lane == ldr) {
@@ -223,80 +348,66 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
           atomicMax(&w.cnt->inv_first_mut, ~first);
         }
         slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, ldr);
+        // same-key mutations of this warp join together: the lowest lane
+        // (lowest op index) joins for all and hands out consecutive
+        // positions in lane order, which is op-index order
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[j]) & mm;
+        const uint32_t lead = is_mut ? __ffs(peers) - 1 : lane;
+        uint32_t gslot = 0, gpos = 0;
+        if (is_mut && lead == lane)
+          gslot = group_join<Tr>(sc, w, i, key[j], h[j], __popc(peers), &gpos);
+        gslot = __shfl_sync(0xFFFFFFFFu, gslot, lead);
+        gpos = __shfl_sync(0xFFFFFFFFu, gpos, lead);
         if (is_mut) {
           sc.mlist[slot_base + __popc(mm & lanemask_lt)] = i;
-          group_join<Tr>(sc, w, i, key, h);
+          group_store<Tr>(sc, w, gslot, gpos + __popc(peers & lanemask_lt), i, loc[j]);
         }
       }
     }
   }
 }
 
-// ---------------------------------------------------------------- phase B
-template <class Tr>
-__device__ void phase_segments(const Scratch& sc, const Window<Tr>& w, uint32_t tid,
-                               uint32_t nthreads) {
-  const uint32_t mcount = ld_cg_u32(&w.cnt->mut_count);
-  for (uint32_t j = tid; j < mcount; j += nthreads) {
-    const uint32_t m = ld_cg_u32(&sc.mlist[j]);
-    const uint64_t mi = ld_cg_u64(&sc.minfo[m]);
-    const uint32_t slot = (uint32_t)(mi >> 32), pos = (uint32_t)mi;
-    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[slot]));
-    if (c == 1) {
-      sc.pred[m] = kPredLast;
-    } else if (pos == 0) {
-      sc.goff[slot] = atomicAdd(&w.cnt->seg_cursor, c);
-      if (c > kSmallGroup) sc.big[atomicAdd(&w.cnt->big_count, 1u)] = slot;
-    }
+// Phase A over the window from op `begin`.  cursor == null or chunk == 0:
+// warp-uniform grid stride of 32*P ops.  Otherwise work is claimed in two
+// levels: a block takes `chunk` consecutive ops with one atomic on *cursor,
+// its warps take 32*P-op tiles of that chunk from a shared counter; blocks
+// that finish early take more chunks (balance without a global atomic per
+// tile).  Every thread of the block must call it.
+template <class Tr, bool kGroup, int P>
+__device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<Tr>& w,
+                            uint32_t warp_id, uint32_t num_warps, uint32_t* cursor,
+                            uint32_t chunk, bool dedup,
+                            ProbeSel sel = ProbeSel{0, 0xFFFFFFFFu, true}, uint32_t begin = 0) {
+  const uint32_t lane = lane_id();
+  if (cursor == nullptr || chunk == 0) {
+    for (uint32_t base = begin + warp_id * 32 * P; base < w.n; base += num_warps * 32 * P)
+      probe_tile<Tr, kGroup, P>(t, sc, w, base, lane, dedup, sel);
+    return;
   }
-}
-
-// ---------------------------------------------------------------- phase C
-template <class Tr>
-__device__ void phase_scatter(const Scratch& sc, const Window<Tr>& w, uint32_t tid,
-                              uint32_t nthreads) {
-  const uint32_t mcount = ld_cg_u32(&w.cnt->mut_count);
-  for (uint32_t j = tid; j < mcount; j += nthreads) {
-    const uint32_t m = ld_cg_u32(&sc.mlist[j]);
-    const uint64_t mi = ld_cg_u64(&sc.minfo[m]);
-    const uint32_t slot = (uint32_t)(mi >> 32), pos = (uint32_t)mi;
-    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[slot]));
-    if (c > 1) sc.seg[ld_cg_u32(&sc.goff[slot]) + pos] = m;
+  __shared__ uint32_t s_base, s_next;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_base = begin + atomicAdd(cursor, chunk);
+      s_next = 0;
+    }
+    __syncthreads();
+    const uint32_t c0 = s_base;
+    if (c0 >= w.n) break;  // block-uniform
+    const uint32_t c1 = min(w.n, c0 + chunk);
+    for (;;) {
+      uint32_t off = 0;
+      if (lane == 0) off = atomicAdd(&s_next, 32u * P);
+      off = __shfl_sync(0xFFFFFFFFu, off, 0);
+      if (c0 + off >= c1) break;
+      probe_tile<Tr, kGroup, P>(t, sc, w, c0 + off, lane, dedup, sel);
+    }
+    __syncthreads();  // s_base / s_next are rewritten next round
   }
 }
 
 // ---------------------------------------------------------------- phase D
-template <class Tr>
-__device__ void phase_sort_small(const Scratch& sc, const Window<Tr>& w, uint32_t tid,
-                                 uint32_t nthreads) {
-  const uint32_t mcount = ld_cg_u32(&w.cnt->mut_count);
-  for (uint32_t j = tid; j < mcount; j += nthreads) {
-    const uint32_t m = ld_cg_u32(&sc.mlist[j]);
-    const uint64_t mi = ld_cg_u64(&sc.minfo[m]);
-    const uint32_t slot = (uint32_t)(mi >> 32), pos = (uint32_t)mi;
-    if (pos != 0) continue;
-    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[slot]));
-    if (c < 2 || c > kSmallGroup) continue;
-    const uint32_t off = ld_cg_u32(&sc.goff[slot]);
-    uint32_t e[kSmallGroup];
-    for (uint32_t a = 0; a < c; ++a) {
-      uint32_t x = ld_cg_u32(&sc.seg[off + a]);
-      uint32_t b = a;
-      while (b > 0 && e[b - 1] > x) {
-        e[b] = e[b - 1];
-        --b;
-      }
-      e[b] = x;
-    }
-    for (uint32_t a = 0; a < c; ++a) {
-      sc.sseg[off + a] = e[a];
-      sc.pred[e[a]] = (a ? e[a - 1] + 1 : 0u) | (a + 1 == c ? kPredLast : 0u);
-    }
-  }
-}
-
-// Block-wide exclusive scan of one value per thread; returns the prefix and
-// the block total.  `tmp` holds one word per warp.
+// Block-wide exclusive scan of one value per thread; `tmp` holds one word per
+// warp.  Returns the prefix; *total receives the block sum.
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* tmp,
                                                          uint32_t* total) {
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -316,7 +427,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
       uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, d);
       if (lane >= (uint32_t)d) s += y;
     }
-    if (lane < nwarps) tmp[lane] = s;  // inclusive warp prefix
+    if (lane < nwarps) tmp[lane] = s;
   }
   __syncthreads();
   uint32_t warp_base = warp ? tmp[warp - 1] : 0;
@@ -325,89 +436,216 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
   return warp_base + x - v;
 }
 
-// Sort the segments of big groups: each block takes groups from the list and
-// orders their op indices by a bitmap counting sort in shared memory, chunk by
-// chunk over the index range.  `smem` holds 2 * kSortChunkWords words.
+// Counting sort of op indices by a bitmap over their range [lo, hi], in
+// passes of kSortChunkWords words; `get(j)` yields member j (< w.n) or an
+// out-of-range value to skip.  Writes the sorted list to seg[off ..].
+template <class Tr, class Get>
+__device__ void bitmap_sort(const Scratch& sc, const Window<Tr>& w, uint32_t c, uint32_t off,
+                            uint32_t* bits, uint32_t* pre, Get get, uint32_t* sorted) {
+  __shared__ uint32_t s_lo, s_hi, s_tmp[32];
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  uint32_t lo = 0xFFFFFFFFu, hi = 0;
+  for (uint32_t j = tid; j < c; j += nt) {
+    const uint32_t x = get(j);
+    if (x >= w.n) continue;  // never stored: skip rather than index with it
+    lo = min(lo, x);
+    hi = max(hi, x);
+  }
+  lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+  hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+  if (tid == 0) {
+    s_lo = 0xFFFFFFFFu;
+    s_hi = 0;
+  }
+  __syncthreads();
+  if ((tid & 31) == 0) {
+    atomicMin(&s_lo, lo);
+    atomicMax(&s_hi, hi);
+  }
+  __syncthreads();
+  lo = s_lo;
+  hi = s_hi;
+  __syncthreads();
+  uint32_t rank_base = 0;
+  const uint32_t span = kSortChunkWords * 32;
+  for (uint32_t cl = lo; cl <= hi; cl += span) {
+    const uint32_t words = min(kSortChunkWords, ((hi - cl) >> 5) + 1);
+    for (uint32_t k = tid; k < words; k += nt) bits[k] = 0;
+    __syncthreads();
+    for (uint32_t j = tid; j < c; j += nt) {
+      const uint32_t x = get(j);
+      if (x <= hi && x >= cl && x - cl < span) atomicOr(&bits[(x - cl) >> 5], 1u << ((x - cl) & 31));
+    }
+    __syncthreads();
+    const uint32_t per = (words + nt - 1) / nt;
+    const uint32_t w0 = tid * per;
+    uint32_t local = 0;
+    for (uint32_t k = 0; k < per; ++k)
+      if (w0 + k < words) local += __popc(bits[w0 + k]);
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(local, s_tmp, &total);
+    for (uint32_t k = 0; k < per; ++k) {
+      if (w0 + k < words) {
+        pre[w0 + k] = run;
+        run += __popc(bits[w0 + k]);
+      }
+    }
+    __syncthreads();
+    for (uint32_t j = tid; j < c; j += nt) {
+      const uint32_t x = get(j);
+      if (x <= hi && x >= cl && x - cl < span) {
+        const uint32_t d = x - cl, wd = d >> 5;
+        const uint32_t r = rank_base + pre[wd] + __popc(bits[wd] & ((1u << (d & 31)) - 1u));
+        sc.seg[off + r] = x;
+        if (sorted) sorted[r] = x;
+      }
+    }
+    rank_base += total;
+    __syncthreads();
+    if (hi - cl < span) break;
+  }
+}
+
+// A group of more than kWarpSort members, ordered by the whole block.  Up to
+// kSortSmall members are gathered into shared memory first (a warp per
+// storage unit: the inline part, then each 32-member chunk with one
+// chunk-table lookup), so the counting sort reads only shared memory.
+template <class Tr>
+__device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_t gslot,
+                                 uint32_t c, uint32_t off, uint32_t* smem) {
+  uint32_t* sorted = smem + kSortSmall;
+  uint32_t* bits = sorted + kSortSmall;
+  uint32_t* pre = bits + kSortChunkWords;
+  if (c <= kSortSmall) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t nchunks = (c - kInline + kChunk - 1) / kChunk;  // <= kSortSmall / kChunk
+    // all chunk-table lookups in flight at once (one per thread), parked in
+    // the prefix area; then each warp copies its chunks, loads issued before
+    // any store so they overlap
+    for (uint32_t k = tid; k < nchunks; k += blockDim.x) pre[k] = chunk_find(sc, w.epoch, gslot, k);
+    if (tid < kInline) smem[tid] = ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + tid]);
+    for (uint32_t j = tid; j < c; j += blockDim.x) sorted[j] = 0xFFFFFFFFu;  // holes stay invalid
+    __syncthreads();
+    for (uint32_t k0 = warp; k0 < nchunks; k0 += 4 * nwarps) {
+      uint32_t v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t k = k0 + q * nwarps;
+        const uint32_t j = kInline + k * kChunk + lane;
+        const uint32_t cs = k < nchunks ? pre[k] : 0xFFFFFFFFu;
+        v[q] = (j < c && cs != 0xFFFFFFFFu) ? ld_cg_u32(&sc.cdat[(size_t)cs * kChunk + lane])
+                                            : 0xFFFFFFFFu;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t j = kInline + (k0 + q * nwarps) * kChunk + lane;
+        if (j < c) smem[j] = v[q];
+      }
+    }
+    __syncthreads();
+    bitmap_sort<Tr>(sc, w, c, off, bits, pre, [&](uint32_t j) { return smem[j]; }, sorted);
+    // every member's predecessor from the sorted list in shared memory (the
+    // bitmap pass ends with a __syncthreads)
+    for (uint32_t j = tid; j < c; j += blockDim.x) {
+      const uint32_t e = sorted[j];
+      const uint32_t pe = j ? sorted[j - 1] : 0xFFFFFFFFu;
+      const uint32_t p = pe < w.n ? pe + 1 : 0u;
+      if (e < w.n) sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
+    }
+    __syncthreads();
+    return;
+  }
+  bitmap_sort<Tr>(sc, w, c, off, bits, pre,
+                  [&](uint32_t j) { return member_at(sc, w.epoch, gslot, j); }, nullptr);
+  __threadfence_block();
+  __syncthreads();
+  // every member's predecessor; op indices read back from scratch are checked
+  // before use as addresses
+  for (uint32_t j = threadIdx.x; j < c; j += blockDim.x) {
+    const uint32_t e = ld_cg_u32(&sc.seg[off + j]);
+    const uint32_t pe = j ? ld_cg_u32(&sc.seg[off + j - 1]) : 0xFFFFFFFFu;
+    const uint32_t p = pe < w.n ? pe + 1 : 0u;
+    if (e < w.n) sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
+  }
+  __syncthreads();
+}
+
+// A group of kInline+1 .. kWarpSort members, ordered by one warp: each lane
+// holds members lane and lane+32 and ranks them against all others by
+// shuffles, tracking its predecessor (the largest smaller index) on the way.
+template <class Tr>
+__device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t gslot, uint32_t c,
+                                uint32_t off) {
+  const uint32_t lane = lane_id();
+  uint32_t x[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t j = lane + 32 * h;
+    x[h] = j < c ? member_at(sc, w.epoch, gslot, j) : 0xFFFFFFFFu;
+  }
+  uint32_t rank[2] = {0, 0}, pred[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    for (uint32_t q = 0; q < 32; ++q) {
+      const uint32_t y = __shfl_sync(0xFFFFFFFFu, x[h], q);
+#pragma unroll
+      for (int g = 0; g < 2; ++g) {
+        if (32 * h + q < c && y < x[g]) {
+          ++rank[g];
+          if (pred[g] == 0xFFFFFFFFu || y > pred[g]) pred[g] = y;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const uint32_t j = lane + 32 * g;
+    if (j < c && x[g] < w.n) {
+      sc.seg[off + rank[g]] = x[g];
+      sc.pred[x[g]] = (pred[g] < w.n ? pred[g] + 1 : 0u) | (rank[g] + 1 == c ? kPredLast : 0u);
+    }
+  }
+}
+
+// Phase D: blocks first take the large groups (the critical path), then each
+// warp takes the remaining groups of the big list.  `smem` holds
+// kSortSmemBytes.
 template <class Tr>
 __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
-  __shared__ uint32_t s_job, s_lo, s_hi, s_tmp[32];
-  uint32_t* bits = smem;
-  uint32_t* pre = smem + kSortChunkWords;
-  const uint32_t tid = threadIdx.x, nt = blockDim.x;
-  const uint32_t nbig = ld_cg_u32(&w.cnt->big_count);
+  __shared__ uint32_t s_job, s_off;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t nlarge = ld_cg_u32(&w.cnt->large_count);
   for (;;) {
-    if (tid == 0) s_job = atomicAdd(&w.cnt->big_work, 1u);
+    if (tid == 0) s_job = atomicAdd(&w.cnt->large_work, 1u);
     __syncthreads();
     const uint32_t job = s_job;
-    if (job >= nbig) break;
-    const uint32_t slot = ld_cg_u32(&sc.big[job]);
-    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[slot]));
-    const uint32_t off = ld_cg_u32(&sc.goff[slot]);
-    uint32_t lo = 0xFFFFFFFFu, hi = 0;
-    for (uint32_t j = tid; j < c; j += nt) {
-      uint32_t x = ld_cg_u32(&sc.seg[off + j]);
-      lo = min(lo, x);
-      hi = max(hi, x);
-    }
-    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
-    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if (job >= nlarge) break;
+    const uint32_t gslot = ld_cg_u32(&sc.large[job]) & sc.gmask;
+    const uint32_t c = min(g_count(ld_relaxed_u64(&sc.gtab[gslot])), w.n);
     if (tid == 0) {
-      s_lo = 0xFFFFFFFFu;
-      s_hi = 0;
+      s_off = atomicAdd(&w.cnt->seg_cursor, c);
+      sc.goff[gslot] = s_off;
     }
     __syncthreads();
-    if ((tid & 31) == 0) {
-      atomicMin(&s_lo, lo);
-      atomicMax(&s_hi, hi);
+    sort_group_block<Tr>(sc, w, gslot, c, s_off, smem);
+  }
+  const uint32_t nbig = ld_cg_u32(&w.cnt->big_count);
+  const uint32_t lane = lane_id();
+  for (;;) {
+    uint32_t job = 0;
+    if (lane == 0) job = atomicAdd(&w.cnt->big_work, 1u);
+    job = __shfl_sync(0xFFFFFFFFu, job, 0);
+    if (job >= nbig) break;
+    const uint32_t gslot = ld_cg_u32(&sc.big[job]) & sc.gmask;
+    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[gslot]));
+    if (c > kWarpSort) continue;  // a block took it
+    uint32_t off = 0;
+    if (lane == 0) {
+      off = atomicAdd(&w.cnt->seg_cursor, c);
+      sc.goff[gslot] = off;
     }
-    __syncthreads();
-    lo = s_lo;
-    hi = s_hi;
-    uint32_t rank_base = 0;
-    const uint32_t span = kSortChunkWords * 32;
-    for (uint32_t cl = lo; cl <= hi; cl += span) {
-      for (uint32_t k = tid; k < kSortChunkWords; k += nt) bits[k] = 0;
-      __syncthreads();
-      for (uint32_t j = tid; j < c; j += nt) {
-        uint32_t x = ld_cg_u32(&sc.seg[off + j]);
-        if (x >= cl && x - cl < span) atomicOr(&bits[(x - cl) >> 5], 1u << ((x - cl) & 31));
-      }
-      __syncthreads();
-      // each thread owns a contiguous run of words
-      const uint32_t per = (kSortChunkWords + nt - 1) / nt;
-      const uint32_t w0 = tid * per;
-      uint32_t local = 0;
-      for (uint32_t k = 0; k < per; ++k)
-        if (w0 + k < kSortChunkWords) local += __popc(bits[w0 + k]);
-      uint32_t total;
-      uint32_t run = block_exclusive_scan(local, s_tmp, &total);
-      for (uint32_t k = 0; k < per; ++k) {
-        if (w0 + k < kSortChunkWords) {
-          pre[w0 + k] = run;
-          run += __popc(bits[w0 + k]);
-        }
-      }
-      __syncthreads();
-      for (uint32_t j = tid; j < c; j += nt) {
-        uint32_t x = ld_cg_u32(&sc.seg[off + j]);
-        if (x >= cl && x - cl < span) {
-          uint32_t d = x - cl, wd = d >> 5;
-          uint32_t r = rank_base + pre[wd] + __popc(bits[wd] & ((1u << (d & 31)) - 1u));
-          sc.sseg[off + r] = x;
-        }
-      }
-      rank_base += total;
-      __syncthreads();
-      if (hi - cl < span) break;  // last chunk (also guards cl overflow)
-    }
-    __threadfence_block();
-    __syncthreads();
-    for (uint32_t j = tid; j < c; j += nt) {
-      uint32_t e = ld_cg_u32(&sc.sseg[off + j]);
-      uint32_t p = j ? ld_cg_u32(&sc.sseg[off + j - 1]) + 1 : 0u;
-      sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
-    }
-    __syncthreads();
+    off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    sort_group_warp<Tr>(sc, w, gslot, c, off);
   }
 }
 
@@ -421,25 +659,59 @@ __device__ __forceinline__ void post_state(const Window<Tr>& w, uint32_t p, bool
   *value = (Tr::kHasValue && pt == kOpWrite) ? val_of(w, p) : 0ull;
 }
 
+// Inline members of a small group: predecessor of op i (or 0xFFFFFFFF) and
+// whether i is the group's last mutation.
+__device__ __forceinline__ uint32_t inline_pred(const Scratch& sc, uint32_t gslot, uint32_t c,
+                                                uint32_t i, uint32_t n, bool* last) {
+  const uint4 a = ld_cg_v4(&sc.ginl[(size_t)gslot * kInline]);
+  const uint4 b = ld_cg_v4(&sc.ginl[(size_t)gslot * kInline + 4]);
+  const uint32_t m[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  uint32_t best = 0xFFFFFFFFu;
+  bool later = false;
+#pragma unroll
+  for (uint32_t q = 0; q < kInline; ++q) {
+    if (q < c && m[q] < n) {
+      if (m[q] < i && (best == 0xFFFFFFFFu || m[q] > best)) best = m[q];
+      later |= m[q] > i;
+    }
+  }
+  *last = !later;
+  return best;
+}
+
 template <class Tr>
 __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
                                         const Window<Tr>& w, uint32_t tid, uint32_t nthreads) {
   const uint32_t mcount = ld_cg_u32(&w.cnt->mut_count);
   for (uint32_t j = tid; j < mcount; j += nthreads) {
     const uint32_t m = ld_cg_u32(&sc.mlist[j]);
-    const uint32_t p = ld_cg_u32(&sc.pred[m]);
+    if (m >= w.n) continue;
+    const uint64_t mi = ld_cg_u64(&sc.minfo[m]);
+    const uint32_t gslot = (uint32_t)(mi >> 32) & sc.gmask;
+    const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[gslot]));
     const uint8_t type = op_type(w, m);
-    if (p & kPredMask) {
+    uint32_t pred;
+    bool last = true;
+    if (c == 1) {
+      pred = 0xFFFFFFFFu;
+    } else if (c <= kInline) {
+      pred = inline_pred(sc, gslot, c, m, w.n, &last);
+    } else {
+      const uint32_t p = ld_cg_u32(&sc.pred[m]);
+      pred = (p & kPredMask) ? (p & kPredMask) - 1 : 0xFFFFFFFFu;
+      last = (p & kPredLast) != 0;
+    }
+    if (pred < w.n) {
       bool present;
       uint64_t value;
-      post_state(w, (p & kPredMask) - 1, &present, &value);
+      post_state(w, pred, &present, &value);
       write_result(w, m, type, present, value);
     }
-    if (p & kPredLast) {
+    if (last) {
       const typename Tr::Key key = key_of(w, m);
       const bool present = type == kOpWrite;
       const uint64_t val = (Tr::kHasValue && present) ? val_of(w, m) : 0ull;
-      table_apply<Tr>(t, key, Tr::hash(key), present, val);
+      table_apply_known<Tr>(t, key, Tr::hash(key), ld_cg_u64(&sc.mloc[m]), present, val);
     }
   }
 }
@@ -454,7 +726,7 @@ __device__ void phase_resolve_reads(const Scratch& sc, const Window<Tr>& w, uint
     if (type != kOpRead) continue;
     const typename Tr::Key key = key_of(w, i);
     const uint64_t h = Tr::hash(key);
-    uint32_t slot = (uint32_t)(h >> 20) & sc.gmask;
+    uint32_t slot = gslot_of(h, sc.gmask);
     uint64_t v = 0;
     bool hit = false;
     for (uint32_t probe = 0; probe <= sc.gmask; ++probe) {
@@ -469,22 +741,23 @@ __device__ void phase_resolve_reads(const Scratch& sc, const Window<Tr>& w, uint
     if (!hit) continue;
     const uint32_t c = g_count(v);
     uint32_t pred_op = 0xFFFFFFFFu;
-    if (c == 1) {
-      const uint32_t o = g_owner(v) - 1;
-      if (o < i) pred_op = o;
+    if (c <= kInline) {
+      bool last;
+      pred_op = inline_pred(sc, slot, c, i, w.n, &last);
     } else {
       const uint32_t off = ld_cg_u32(&sc.goff[slot]);
-      uint32_t lo = 0, hi = c;  // count of entries < i
+      if (off > sc.max_window || c > sc.max_window - off) continue;
+      uint32_t lo = 0, hi = c;  // count of members < i
       while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (ld_cg_u32(&sc.sseg[off + mid]) < i)
+        if (ld_cg_u32(&sc.seg[off + mid]) < i)
           lo = mid + 1;
         else
           hi = mid;
       }
-      if (lo > 0) pred_op = ld_cg_u32(&sc.sseg[off + lo - 1]);
+      if (lo > 0) pred_op = ld_cg_u32(&sc.seg[off + lo - 1]);
     }
-    if (pred_op != 0xFFFFFFFFu) {
+    if (pred_op < w.n) {
       bool present;
       uint64_t value;
       post_state(w, pred_op, &present, &value);
