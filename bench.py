@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--chunk", type=int, default=-1)
     ap.add_argument("--dedup", type=int, default=-1)
     ap.add_argument("--split", type=int, default=-1, help="fused: percent of reads probed first")
+    ap.add_argument("--region", type=int, default=-1, help="fused: probe in table-region order")
     ap.add_argument("--trace", action="store_true", help="single mode: print fused phase times")
     ap.add_argument("--single", action="store_true",
                     help="fused timing only (one table, no plain/e2e/cpu legs): the small "
@@ -208,6 +209,8 @@ def apply_tuning(args, table):
         kw["dedup"] = args.dedup
     if args.split >= 0:
         kw["fused_split"] = args.split
+    if args.region >= 0:
+        kw["region_order"] = args.region
     if kw:
         table.set_tuning(**kw)
 

@@ -92,6 +92,7 @@ typedef struct lsb_tuning {
   uint32_t dedup;         /* 1: lanes of a warp carrying the same key share one lookup */
   uint32_t fused_split;   /* fused path: percent of a window's reads probed before the
                              same-key ordering pass (the rest run during it), 0..100 */
+  uint32_t region_order;  /* fused path: 1 = probe a window in table-region order */
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */

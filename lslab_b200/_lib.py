@@ -57,6 +57,7 @@ class Tuning(C.Structure):
         ("prefetch", C.c_uint32),
         ("dedup", C.c_uint32),
         ("fused_split", C.c_uint32),
+        ("region_order", C.c_uint32),
     ]
 
 

@@ -19,6 +19,11 @@ namespace {
 constexpr uint32_t kDefaultWindow = 1u << 20;
 constexpr uint32_t kMaxWindow = 1u << 23;  // owner field of a group slot is 24 bits
 constexpr uint32_t kTraceCap = 1024;        // phase-trace entries per fused launch
+// One allocation for everything a fused launch zeroes first: two window
+// counter sets, the grid barrier, two region-counter sets.
+constexpr size_t kBinsOffset = 256;
+constexpr size_t kCounterBytes = kBinsOffset + 2 * sizeof(BinCounters);
+static_assert(2 * sizeof(WinCounters) + sizeof(GridBarrier) <= kBinsOffset, "counter block");
 
 // Device arrays must be naturally aligned for their element type; a
 // misaligned device access would fault the context, so it is refused here.
@@ -65,6 +70,9 @@ struct FusedJob {
   uint32_t dedup;
   uint32_t split_q16;  // fraction of reads probed with the mutations (x 65536)
   uint64_t* trace;     // optional: phase-boundary timestamps (ns), block 0 records
+  BinCounters* bins;   // two sets, by window parity
+  uint32_t binned;     // probe in table-region order
+  uint32_t bin_shift;  // bucket index >> bin_shift = region
 };
 
 // Phase trace: entry = globaltimer ns << 8 | window & 0x3F << 2 | phase (0 start,
@@ -99,14 +107,23 @@ __global__ void __launch_bounds__(1024, 1)
     }
     w.epoch = job.epoch0 + wi;
     w.cnt = &sc.cnt[wi & 1];
-    // the other counter set was last read in window wi-1, which has ended
+    // the other counter sets were last read in window wi-1, which has ended
     if (tid == 0) win_counters_reset(&sc.cnt[(wi + 1) & 1]);
+    if (tid < 2 * kBins) (&job.bins[(wi + 1) & 1].count[0])[tid] = 0;
+    const uint32_t* perm = nullptr;
+    if (job.binned) {
+      phase_bin_count<Tr>(t, w, sc.obin, &job.bins[wi & 1], job.bin_shift);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+      phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+      perm = sc.perm;
+    }
     // Reads [0, split) are probed with the mutations; reads [split, n) in the
     // sort pass, where they fill the SMs that the (latency-bound, few-block)
     // ordering of big groups leaves idle.  Reads do not depend on the groups.
     const uint32_t split = (uint32_t)(((uint64_t)w.n * job.split_q16) >> 16);
     phase_probe<Tr, true, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, job.chunk,
-                             job.dedup != 0, ProbeSel{0, split, true});
+                             job.dedup != 0, ProbeSel{0, split, true}, 0, perm);
     if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     trace_mark(job.trace, tat, wi, 1);
     // counters read after the barrier: the same values in every block, so the
@@ -118,7 +135,7 @@ __global__ void __launch_bounds__(1024, 1)
       if (split < w.n)  // small claims so blocks freed by the sort take more
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
                                   blockDim.x * P, job.dedup != 0, ProbeSel{split, w.n, false},
-                                  split & ~31u);
+                                  split & ~31u, perm);
       if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     }
     trace_mark(job.trace, tat, wi, 2);
@@ -193,7 +210,7 @@ inline bool tuning_ok(const lsb_tuning& x) {
   return (x.block_threads == 128 || x.block_threads == 256 || x.block_threads == 512 ||
           x.block_threads == 1024) &&
          x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
-         x.fused_split <= 100;
+         x.fused_split <= 100 && x.region_order <= 1;
 }
 
 template <class Tr>
@@ -215,6 +232,8 @@ struct Table {
   Tuning tune;
   uint32_t split_q16 = 65536;  // all of a window's reads probed before the sort pass
   uint64_t* trace = nullptr;   // device phase-trace buffer when tracing is on
+  BinCounters* bins = nullptr; // inside the counter block (see kCounterBytes)
+  bool binned = false;         // fused path probes in table-region order (measured slower)
   int fused_per_sm[3][4] = {};  // occupancy by (prefetch, block size) once queried
 
   TableView view() const {
@@ -232,7 +251,7 @@ struct Table {
   void release() {
     void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
-                    sc.cnt, trace};
+                    sc.cnt, sc.obin, sc.perm, trace};
     for (void* p : ptrs) cudaFree(p);
   }
 
@@ -277,7 +296,9 @@ struct Table {
         cudaMalloc(&sc.mlist, sizeof(uint32_t) * window) == cudaSuccess &&
         cudaMalloc(&sc.big, sizeof(uint32_t) * (window / (kInline + 1) + 1)) == cudaSuccess &&
         cudaMalloc(&sc.large, sizeof(uint32_t) * (window / (kWarpSort + 1) + 1)) == cudaSuccess &&
-        cudaMalloc(&sc.cnt, sizeof(WinCounters) * 2 + sizeof(GridBarrier)) == cudaSuccess;
+        cudaMalloc(&sc.obin, window) == cudaSuccess &&
+        cudaMalloc(&sc.perm, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       return LSB_ERR_OOM;
@@ -291,8 +312,9 @@ struct Table {
     LSB_CK(cudaMemcpy(pool, p.data(), sizeof(uint64_t) * p.size(), cudaMemcpyHostToDevice));
     LSB_CK(cudaMemset(sc.gtab, 0, sizeof(uint64_t) * g));
     LSB_CK(cudaMemset(sc.ctab, 0, sizeof(uint64_t) * cg));
-    LSB_CK(cudaMemset(sc.cnt, 0, sizeof(WinCounters) * 2 + sizeof(GridBarrier)));
+    LSB_CK(cudaMemset(sc.cnt, 0, kCounterBytes));
     bar = reinterpret_cast<GridBarrier*>(sc.cnt + 2);
+    bins = reinterpret_cast<BinCounters*>(reinterpret_cast<uint8_t*>(sc.cnt) + kBinsOffset);
     LSB_CK(cudaFuncSetAttribute(k_sort<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -311,6 +333,7 @@ struct Table {
     tune.prefetch = x.prefetch;
     tune.dedup = x.dedup;
     split_q16 = (uint32_t)(((uint64_t)x.fused_split << 16) / 100);
+    binned = x.region_order != 0;
     return LSB_OK;
   }
 
@@ -320,6 +343,7 @@ struct Table {
     x->prefetch = tune.prefetch;
     x->dedup = tune.dedup;
     x->fused_split = (uint32_t)(((uint64_t)split_q16 * 100 + 32768) >> 16);
+    x->region_order = binned ? 1u : 0u;
   }
 
   // Next epoch for a window; clears the group and chunk tables when the
@@ -438,6 +462,9 @@ struct Table {
     job.dedup = tune.dedup;
     job.split_q16 = split_q16;
     job.trace = trace;
+    job.bins = bins;
+    job.binned = binned ? 1u : 0u;
+    job.bin_shift = log2 > kBinBits ? log2 - kBinBits : 0u;
     if (trace) LSB_CK(cudaMemsetAsync(trace, 0, sizeof(uint64_t) * kTraceCap, s));
     uint32_t nwin = (uint32_t)((n + job.window - 1) / job.window);
     if (nwin > 0xFFF0u) return LSB_ERR_ARG;
@@ -445,8 +472,8 @@ struct Table {
     if (grid <= 0) return LSB_ERR_STATE;
     int e = next_epochs(nwin, s, &job.epoch0);
     if (e) return e;
-    // counters of both windows and the barrier: one memset
-    LSB_CK(cudaMemsetAsync(sc.cnt, 0, sizeof(WinCounters) * 2 + sizeof(GridBarrier), s));
+    // counters of both windows, the barrier and the region counters: one memset
+    LSB_CK(cudaMemsetAsync(sc.cnt, 0, kCounterBytes, s));
     TableView tv = view();
     Scratch scv = sc;
     GridBarrier* b = bar;

@@ -95,6 +95,8 @@ struct Scratch {
   uint32_t* big;    // group slots with more than kInline members
   uint32_t* large;  // group slots with more than kWarpSort members
   WinCounters* cnt; // two sets, used by alternate windows
+  uint8_t* obin;    // per op: table region (binned probing)
+  uint32_t* perm;   // probe position -> op index (binned probing)
 };
 
 enum : uint32_t { kOutNone = 0, kOutResult = 1, kOutOld = 2, kOutBool = 3 };
@@ -284,23 +286,30 @@ struct ProbeSel {
   bool muts;
 };
 
+// `perm` (optional): position -> op index (the binned order); positions
+// base + j*32 + lane are then mapped to ops, and sel's read range is in
+// positions.
 template <class Tr, bool kGroup, int P>
 __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc,
                                            const Window<Tr>& w, uint32_t base, uint32_t lane,
-                                           bool dedup, const ProbeSel& sel) {
+                                           bool dedup, const ProbeSel& sel,
+                                           const uint32_t* perm) {
   using Key = typename Tr::Key;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
   Key key[P];
   uint64_t h[P], value[P], loc[P];
   uint8_t type[P];
   bool active[P], want[P], found[P];
-  uint32_t src[P];
+  uint32_t src[P], idx[P];
 #pragma unroll
   for (int j = 0; j < P; ++j) {
-    const uint32_t i = base + j * 32 + lane;
-    type[j] = i < w.n ? op_type_stream(w, i) : kOpRead;
-    active[j] = i < w.n && (type[j] == kOpRead ? (i >= sel.read_lo && i < sel.read_hi) : sel.muts);
-    key[j] = active[j] ? key_stream(w, i) : (Key)0;
+    const uint32_t pos = base + j * 32 + lane;
+    uint32_t i = pos;
+    if (perm != nullptr && pos < w.n) i = min(ld_cs_u32(perm + pos), w.n);
+    idx[j] = i;
+    type[j] = i < w.n ? (perm ? op_type(w, i) : op_type_stream(w, i)) : kOpRead;
+    active[j] = i < w.n && (type[j] == kOpRead ? (pos >= sel.read_lo && pos < sel.read_hi) : sel.muts);
+    key[j] = active[j] ? (perm ? key_of(w, i) : key_stream(w, i)) : (Key)0;
     h[j] = Tr::hash(key[j]);
     want[j] = active[j];
     src[j] = lane;
@@ -334,7 +343,7 @@ __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc
       value[j] = __shfl_sync(0xFFFFFFFFu, value[j], src[j]);
       loc[j] = __shfl_sync(0xFFFFFFFFu, loc[j], src[j]);
     }
-    const uint32_t i = base + j * 32 + lane;
+    const uint32_t i = idx[j];
     if (active[j]) write_result(w, i, type[j], found[j], value[j]);
     if (kGroup) {
       const bool is_mut = active[j] && type[j] != kOpRead;
@@ -377,11 +386,12 @@ template <class Tr, bool kGroup, int P>
 __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<Tr>& w,
                             uint32_t warp_id, uint32_t num_warps, uint32_t* cursor,
                             uint32_t chunk, bool dedup,
-                            ProbeSel sel = ProbeSel{0, 0xFFFFFFFFu, true}, uint32_t begin = 0) {
+                            ProbeSel sel = ProbeSel{0, 0xFFFFFFFFu, true}, uint32_t begin = 0,
+                            const uint32_t* perm = nullptr) {
   const uint32_t lane = lane_id();
   if (cursor == nullptr || chunk == 0) {
     for (uint32_t base = begin + warp_id * 32 * P; base < w.n; base += num_warps * 32 * P)
-      probe_tile<Tr, kGroup, P>(t, sc, w, base, lane, dedup, sel);
+      probe_tile<Tr, kGroup, P>(t, sc, w, base, lane, dedup, sel, perm);
     return;
   }
   __shared__ uint32_t s_base, s_next;
@@ -399,9 +409,78 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
       if (lane == 0) off = atomicAdd(&s_next, 32u * P);
       off = __shfl_sync(0xFFFFFFFFu, off, 0);
       if (c0 + off >= c1) break;
-      probe_tile<Tr, kGroup, P>(t, sc, w, c0 + off, lane, dedup, sel);
+      probe_tile<Tr, kGroup, P>(t, sc, w, c0 + off, lane, dedup, sel, perm);
     }
     __syncthreads();  // s_base / s_next are rewritten next round
+  }
+}
+
+// --------------------------------------------------------- region binning
+// Random probes over a multi-GB table are limited by address translation:
+// measured on B200, random 32-B reads over 4 GB run at ~19 G/s, but at ~48 G/s
+// when each block stays inside a 32 MB region.  The fused path therefore
+// probes a window in table-region order: ops are counted per region (the top
+// kBinBits of the bucket index: consecutive slabs), then their indices are
+// scattered into region order (perm), and the probe walks perm, so at any
+// moment the grid works within one or two regions.  Each op still writes
+// its own result; only the probing order changes.
+constexpr uint32_t kBinBits = 6;
+constexpr uint32_t kBins = 1u << kBinBits;
+
+struct BinCounters {
+  uint32_t count[kBins];
+  uint32_t cursor[kBins];
+};
+
+// Pass 1: per-op region (stored, one byte) and per-region counts.
+template <class Tr>
+__device__ void phase_bin_count(const TableView& t, const Window<Tr>& w, uint8_t* obin,
+                                BinCounters* bc, uint32_t shift) {
+  __shared__ uint32_t hist[kBins];
+  for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  const uint32_t nt = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt) {
+    const uint32_t b = ((uint32_t)Tr::hash(key_stream(w, i)) & t.mask) >> shift;
+    obin[i] = (uint8_t)b;
+    atomicAdd(&hist[b], 1u);
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x)
+    if (hist[b]) atomicAdd(&bc->count[b], hist[b]);
+}
+
+// Pass 2: each block reserves a range per region for the ops it counted in
+// pass 1 (same grid-stride mapping, so the same ops) and writes their indices
+// there.
+template <class Tr>
+__device__ void phase_bin_scatter(const Window<Tr>& w, const uint8_t* obin, uint32_t* perm,
+                                  BinCounters* bc) {
+  __shared__ uint32_t hist[kBins], base[kBins];
+  for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  const uint32_t nt = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt)
+    atomicAdd(&hist[obin[i] & (kBins - 1)], 1u);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // region starts: exclusive scan of the 64 counts
+    const uint32_t lane = threadIdx.x;
+    const uint32_t c0 = ld_cg_u32(&bc->count[2 * lane]), c1 = ld_cg_u32(&bc->count[2 * lane + 1]);
+    uint32_t x = c0 + c1;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+      if (lane >= (uint32_t)d) x += y;
+    }
+    const uint32_t start0 = x - c0 - c1;
+    const uint32_t h0 = hist[2 * lane], h1 = hist[2 * lane + 1];
+    base[2 * lane] = start0 + (h0 ? atomicAdd(&bc->cursor[2 * lane], h0) : 0u);
+    base[2 * lane + 1] = start0 + c0 + (h1 ? atomicAdd(&bc->cursor[2 * lane + 1], h1) : 0u);
+  }
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt) {
+    const uint32_t pos = atomicAdd(&base[obin[i] & (kBins - 1)], 1u);
+    if (pos < w.n) perm[pos] = i;
   }
 }
 
