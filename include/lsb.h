@@ -173,6 +173,17 @@ int lsb_map_pool_usage(lsb_map* m, uint64_t* used, uint64_t* capacity, cudaStrea
 /* Number of live entries (synchronises the stream). */
 int lsb_map_size(lsb_map* m, uint64_t* count, cudaStream_t stream);
 
+/* Number of live entries, written to *count_out, a DEVICE word the caller
+ * provides, asynchronously on `stream`, without allocating any memory (no
+ * counterpart in the reference: it is the allocation-free form of
+ * lsb_map_size for callers that must not allocate, e.g. while recording a
+ * stream capture or under a fully pre-reserved memory budget).  Its scratch is
+ * one static device array shared by all calls: maps of at most 2^20 buckets
+ * (larger ones return LSB_ERR_ARG); calls that overlap on the GPU race on the
+ * array; the first call on each device resolves the array's address and
+ * should come before any stream capture. */
+int lsb_map_size_noalloc(lsb_map* m, uint64_t* count_out, cudaStream_t stream);
+
 /* Copy every live (key, value) pair to HOST arrays, in key order.  *count
  * receives the number of live entries; at most cap pairs are written.
  * Synchronises the stream. */

@@ -87,6 +87,7 @@ _SIGS = {
     "lsb_map_status": (C.c_int, [_P, C.POINTER(_U32), _P]),
     "lsb_map_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
     "lsb_map_size": (C.c_int, [_P, C.POINTER(_U64), _P]),
+    "lsb_map_size_noalloc": (C.c_int, [_P, _P, _P]),
     "lsb_map_dump": (C.c_int, [_P, _P, _P, _SZ, C.POINTER(_U64), _P]),
     "lsb_set_create": (C.c_int, [C.c_uint, _U64, C.POINTER(_P)]),
     "lsb_set_create_ex": (C.c_int, [C.c_uint, C.POINTER(Options), C.POINTER(_P)]),

@@ -601,6 +601,13 @@ struct lsb_set {
   Table<SetTraits> t;
 };
 
+// Internal accessor for other translation units of the library (see
+// lsb_internal.h): the device view and bucket count of a map.
+void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buckets) {
+  *view = m->t.view();
+  *buckets = m->t.buckets;
+}
+
 extern "C" {
 
 // ------------------------------------------------------------------ map

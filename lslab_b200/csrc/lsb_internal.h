@@ -1,0 +1,10 @@
+// Declarations shared between the library's translation units (not part of
+// the public C-ABI).
+#pragma once
+
+#include <cstdint>
+
+#include "lsb.h"
+#include "lsb_core.cuh"
+
+void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buckets);
