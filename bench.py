@@ -160,25 +160,21 @@ def dist_setup(args):
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from lslab_b200.shard import max_over_ranks as mor
+    return mor(x) if world > 1 else x
 
 
 def barrier(world: int):
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        from lslab_b200.shard import barrier as b
+        b()
 
 
 # ------------------------------------------------------------------ workload
 def make_batches(args, rank: int, count: int):
     from lslab_b200 import workload as W
-    seed = args.seed + 1000 * rank
+    from lslab_b200.shard import rank_seed
+    seed = rank_seed(args.seed, rank)
     n = 1 << args.batch_log2
     items = 1 << args.prefill_log2
     return [W.map_zipf_batch(seed, b, n, items, args.theta, (1 - args.put_frac, args.put_frac))
@@ -187,7 +183,8 @@ def make_batches(args, rank: int, count: int):
 
 def prefill_arrays(args, rank: int):
     from lslab_b200 import workload as W
-    seed = args.seed + 1000 * rank
+    from lslab_b200.shard import rank_seed
+    seed = rank_seed(args.seed, rank)
     keys = W.prefill_keys(seed, 1 << args.prefill_log2)
     return keys, W.prefill_values(keys)
 

@@ -228,6 +228,39 @@ int lsb_set_size(lsb_set* s, uint64_t* count, cudaStream_t stream);
 int lsb_set_dump(lsb_set* s, uint32_t* keys_out, size_t cap, uint64_t* count,
                  cudaStream_t stream);
 
+/* ---- batching: CUDA graphs and the autotuner ---------------------------
+ * No reference counterpart (the reference launches one kernel per op-type
+ * batch, include/lslab/map.h:189-220).  A batch may be any concatenation of
+ * smaller batches: results equal running them one after another. */
+typedef struct lsb_graph lsb_graph;
+
+/* Capture lsb_map_execute_fused on these buffers into an instantiated CUDA
+ * graph (one memset and one cooperative kernel).  Each lsb_graph_launch runs
+ * the batch currently in the buffers; the window epochs live on the device,
+ * so replays never reuse one. */
+int lsb_map_capture_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys,
+                          const uint64_t* vals, lsb_result* out, size_t n, lsb_graph** graph);
+int lsb_set_capture_fused(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool* out,
+                          size_t n, lsb_graph** graph);
+int lsb_graph_launch(lsb_graph* g, cudaStream_t stream);
+int lsb_graph_destroy(lsb_graph* g);
+
+/* Autotuner: times the fused path on a sample batch for every block size
+ * (256, 512, 1024 threads = 8, 16, 32 warps), probe claim size (static, 1024,
+ * 2048, 4096 ops) and lookahead (0, 1, 2), keeps the fastest on the table
+ * and in a process-wide cache by table size that tables created later with
+ * the same log2_buckets start from.  The sample is applied once per
+ * candidate: the final table contents equal one application (a key's final
+ * state is its last mutation in the batch), `out` is scratch.  Synchronises
+ * the stream. */
+int lsb_map_autotune(lsb_map* m, const uint8_t* types, const uint64_t* keys,
+                     const uint64_t* vals, lsb_result* out, size_t n, cudaStream_t stream,
+                     lsb_tuning* best);
+int lsb_set_autotune(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool* out,
+                     size_t n, cudaStream_t stream, lsb_tuning* best);
+/* container: 0 map, 1 set.  LSB_ERR_STATE when that size was never tuned. */
+int lsb_autotune_lookup(int container, unsigned log2_buckets, lsb_tuning* out);
+
 /* ---- misc ------------------------------------------------------------- */
 const char* lsb_error_string(int code);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */

@@ -145,6 +145,29 @@ class _Table:
         self._call("read_trace", buf.ctypes.data, len(buf), C.byref(n), _stream(stream))
         return [(int(x) >> 8, (int(x) >> 2) & 0x3F, int(x) & 3) for x in buf[: n.value]]
 
+    def autotune(self, types, keys, values, output, size=None, stream=None) -> dict:
+        """Sweep the fused path's launch shape on a sample batch (see lsb.h);
+        returns the chosen tuning."""
+        t = _lib.Tuning()
+        if self._prefix == "map":
+            self._call("autotune", _ptr(types), _ptr(keys), _ptr(values), _ptr(output),
+                       _len(keys, size), _stream(stream), C.byref(t))
+        else:
+            self._call("autotune", _ptr(types), _ptr(keys), _ptr(output), _len(keys, size),
+                       _stream(stream), C.byref(t))
+        return {f: int(getattr(t, f)) for f, _ in _lib.Tuning._fields_}
+
+    def capture_fused(self, types, keys, values, output, size=None) -> "Graph":
+        """CUDA graph of execute_fused on these buffers (replay with .launch())."""
+        g = C.c_void_p()
+        if self._prefix == "map":
+            self._call("capture_fused", _ptr(types), _ptr(keys), _ptr(values), _ptr(output),
+                       _len(keys, size), C.byref(g))
+        else:
+            self._call("capture_fused", _ptr(types), _ptr(keys), _ptr(output), _len(keys, size),
+                       C.byref(g))
+        return Graph(g)
+
     def tuning(self) -> dict:
         t = _lib.Tuning()
         self._call("get_tuning", C.byref(t))
@@ -155,6 +178,27 @@ class _Table:
         cur.update(kw)
         t = _lib.Tuning(**cur)
         self._call("set_tuning", C.byref(t))
+
+
+class Graph:
+    """A captured fused launch (lsb_graph)."""
+
+    def __init__(self, handle):
+        self._g = handle
+
+    def launch(self, stream=None):
+        _lib.check(lib().lsb_graph_launch(self._g, _stream(stream)), "lsb_graph_launch")
+
+    def close(self):
+        if self._g is not None and self._g.value:
+            lib().lsb_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Map(_Table):

@@ -106,6 +106,13 @@ _SIGS = {
     "lsb_set_pool_usage": (C.c_int, [_P, C.POINTER(_U64), C.POINTER(_U64), _P]),
     "lsb_set_size": (C.c_int, [_P, C.POINTER(_U64), _P]),
     "lsb_set_dump": (C.c_int, [_P, _P, _SZ, C.POINTER(_U64), _P]),
+    "lsb_map_autotune": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P, C.POINTER(Tuning)]),
+    "lsb_set_autotune": (C.c_int, [_P, _P, _P, _P, _SZ, _P, C.POINTER(Tuning)]),
+    "lsb_autotune_lookup": (C.c_int, [C.c_int, C.c_uint, C.POINTER(Tuning)]),
+    "lsb_map_capture_fused": (C.c_int, [_P, _P, _P, _P, _P, _SZ, C.POINTER(_P)]),
+    "lsb_set_capture_fused": (C.c_int, [_P, _P, _P, _P, _SZ, C.POINTER(_P)]),
+    "lsb_graph_launch": (C.c_int, [_P, _P]),
+    "lsb_graph_destroy": (C.c_int, [_P]),
     "lsb_error_string": (C.c_char_p, [C.c_int]),
     "lsb_version": (C.c_int, []),
 }

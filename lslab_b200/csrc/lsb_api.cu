@@ -4,6 +4,8 @@
 // status word.
 #include <algorithm>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -19,6 +21,8 @@ namespace {
 constexpr uint32_t kDefaultWindow = 1u << 20;
 constexpr uint32_t kMaxWindow = 1u << 23;  // owner field of a group slot is 24 bits
 constexpr uint32_t kTraceCap = 1024;        // phase-trace entries per fused launch
+constexpr uint32_t kFusedEpochs = 32767;    // odd epochs 1..65535 for fused windows
+constexpr uint32_t kPlainEpochs = 32767;    // even epochs 2..65534 for per-phase windows
 // One allocation for everything a fused launch zeroes first: two window
 // counter sets, the grid barrier, two region-counter sets.
 constexpr size_t kBinsOffset = 256;
@@ -65,7 +69,7 @@ template <class Tr>
 struct FusedJob {
   Window<Tr> base;  // whole batch; n = total ops
   uint32_t window;  // ops per window
-  uint32_t epoch0;  // epoch of the first window
+  uint32_t* fused_epoch;  // device: fused windows run so far (epochs of the fused path)
   uint32_t chunk;   // probe work claim size (0 = static stride)
   uint32_t dedup;
   uint32_t split_q16;  // fraction of reads probed with the mutations (x 65536)
@@ -93,6 +97,17 @@ __global__ void __launch_bounds__(1024, 1)
   const uint32_t warp = tid >> 5, nwarps = nt >> 5;
   const uint32_t nwin = (job.base.n + job.window - 1) / job.window;
   uint32_t tat = 0, seq = 0;
+  // Window epochs live on the device so that a replayed CUDA graph of this
+  // launch never reuses one: the fused path takes odd epochs 2f+1 (f = fused
+  // windows so far), the per-phase path even ones from the host.  When the
+  // 16-bit epoch would wrap, the grid clears the group and chunk tables first.
+  uint32_t f = ld_cg_u32(job.fused_epoch);
+  if (f + nwin > kFusedEpochs) {
+    for (size_t i = tid; i <= sc.gmask; i += nt) sc.gtab[i] = 0;
+    for (size_t i = tid; i <= sc.cmask; i += nt) sc.ctab[i] = 0;
+    f = 0;
+    if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+  }
   for (uint32_t wi = 0; wi < nwin; ++wi) {
     trace_mark(job.trace, tat, wi, 0);
     Window<Tr> w = job.base;
@@ -105,7 +120,7 @@ __global__ void __launch_bounds__(1024, 1)
       size_t esz = w.out_kind == kOutResult ? 16 : (w.out_kind == kOutOld ? 8 : 1);
       w.out = (uint8_t*)w.out + (size_t)start * esz;
     }
-    w.epoch = job.epoch0 + wi;
+    w.epoch = 2 * (f + wi) + 1;
     w.cnt = &sc.cnt[wi & 1];
     // the other counter sets were last read in window wi-1, which has ended
     if (tid == 0) win_counters_reset(&sc.cnt[(wi + 1) & 1]);
@@ -125,6 +140,8 @@ __global__ void __launch_bounds__(1024, 1)
     phase_probe<Tr, true, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, job.chunk,
                              job.dedup != 0, ProbeSel{0, split, true}, 0, perm);
     if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+    // every block has read the epoch counter (before its first barrier)
+    if (wi == 0 && tid == 0) *job.fused_epoch = f + nwin;
     trace_mark(job.trace, tat, wi, 1);
     // counters read after the barrier: the same values in every block, so the
     // skips below are grid-uniform
@@ -199,11 +216,13 @@ __global__ void k_dump(TableView t, uint32_t buckets, typename Tr::Key* keys, ui
 }
 
 // ------------------------------------------------------------- tables
+// Defaults: the best of a sweep on the 2^22-bucket, 95/5 Zipf(0.99) workload
+// (block 512; lookahead and in-warp dedup both measured slower there).
 struct Tuning {
   uint32_t block = 512;  // threads per block (128..1024)
   uint32_t chunk = 0;    // probe work claim (0 = static stride)
-  uint32_t prefetch = 1; // extra lookups in flight per thread (0..2)
-  uint32_t dedup = 1;
+  uint32_t prefetch = 0; // extra lookups in flight per thread (0..2)
+  uint32_t dedup = 0;
 };
 
 inline bool tuning_ok(const lsb_tuning& x) {
@@ -233,6 +252,7 @@ struct Table {
   uint32_t split_q16 = 65536;  // all of a window's reads probed before the sort pass
   uint64_t* trace = nullptr;   // device phase-trace buffer when tracing is on
   BinCounters* bins = nullptr; // inside the counter block (see kCounterBytes)
+  uint32_t* fused_epoch = nullptr;  // device counter of fused windows (see k_fused)
   bool binned = false;         // fused path probes in table-region order (measured slower)
   int fused_per_sm[3][4] = {};  // occupancy by (prefetch, block size) once queried
 
@@ -251,7 +271,7 @@ struct Table {
   void release() {
     void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
-                    sc.cnt, sc.obin, sc.perm, trace};
+                    sc.cnt, sc.obin, sc.perm, trace, fused_epoch};
     for (void* p : ptrs) cudaFree(p);
   }
 
@@ -298,7 +318,8 @@ struct Table {
         cudaMalloc(&sc.large, sizeof(uint32_t) * (window / (kWarpSort + 1) + 1)) == cudaSuccess &&
         cudaMalloc(&sc.obin, window) == cudaSuccess &&
         cudaMalloc(&sc.perm, sizeof(uint32_t) * window) == cudaSuccess &&
-        cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess;
+        cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess &&
+        cudaMalloc(&fused_epoch, sizeof(uint32_t)) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       return LSB_ERR_OOM;
@@ -313,6 +334,7 @@ struct Table {
     LSB_CK(cudaMemset(sc.gtab, 0, sizeof(uint64_t) * g));
     LSB_CK(cudaMemset(sc.ctab, 0, sizeof(uint64_t) * cg));
     LSB_CK(cudaMemset(sc.cnt, 0, kCounterBytes));
+    LSB_CK(cudaMemset(fused_epoch, 0, sizeof(uint32_t)));
     bar = reinterpret_cast<GridBarrier*>(sc.cnt + 2);
     bins = reinterpret_cast<BinCounters*>(reinterpret_cast<uint8_t*>(sc.cnt) + kBinsOffset);
     LSB_CK(cudaFuncSetAttribute(k_sort<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -346,16 +368,16 @@ struct Table {
     x->region_order = binned ? 1u : 0u;
   }
 
-  // Next epoch for a window; clears the group and chunk tables when the
-  // 16-bit epoch wraps.
-  int next_epochs(uint32_t count, cudaStream_t s, uint32_t* first) {
-    if (epoch + count > 0xFFFFu) {
+  // Epoch of the next per-phase window (even: 2, 4, ...; the fused path uses
+  // odd ones on the device); clears the group and chunk tables when they wrap.
+  int next_plain_epoch(cudaStream_t s, uint32_t* e) {
+    if (epoch + 1 > kPlainEpochs) {
       LSB_CK(cudaMemsetAsync(sc.gtab, 0, sizeof(uint64_t) * (sc.gmask + 1ull), s));
       LSB_CK(cudaMemsetAsync(sc.ctab, 0, sizeof(uint64_t) * (sc.cmask + 1ull), s));
       epoch = 0;
     }
-    *first = epoch + 1;
-    epoch += count;
+    epoch += 1;
+    *e = 2 * epoch;
     return LSB_OK;
   }
 
@@ -423,7 +445,7 @@ struct Table {
       Window<Tr> w = window(types ? types + off : nullptr, uniform, keys + off * kstride, kstride,
                             vals ? vals + off * vstride : nullptr, vstride,
                             out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr, out_kind, m);
-      int e = next_epochs(1, s, &w.epoch);
+      int e = next_plain_epoch(s, &w.epoch);
       if (e) return e;
       w.cnt = &sc.cnt[0];
       LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
@@ -467,11 +489,10 @@ struct Table {
     job.bin_shift = log2 > kBinBits ? log2 - kBinBits : 0u;
     if (trace) LSB_CK(cudaMemsetAsync(trace, 0, sizeof(uint64_t) * kTraceCap, s));
     uint32_t nwin = (uint32_t)((n + job.window - 1) / job.window);
-    if (nwin > 0xFFF0u) return LSB_ERR_ARG;
+    if (nwin > kFusedEpochs / 2) return LSB_ERR_ARG;
     const int grid = fused_grid();
     if (grid <= 0) return LSB_ERR_STATE;
-    int e = next_epochs(nwin, s, &job.epoch0);
-    if (e) return e;
+    job.fused_epoch = fused_epoch;
     // counters of both windows, the barrier and the region counters: one memset
     LSB_CK(cudaMemsetAsync(sc.cnt, 0, kCounterBytes, s));
     TableView tv = view();
@@ -594,6 +615,118 @@ struct Table {
 
 }  // namespace
 
+// Tuned launch shapes by (container, log2 buckets), filled by the autotuner;
+// a table created later with the same shape starts from them.
+static std::mutex g_tune_mu;
+static std::map<std::pair<int, unsigned>, lsb_tuning> g_tuned;
+
+static bool tuned_lookup(int kind, unsigned log2, lsb_tuning* out) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tuned.find({kind, log2});
+  if (it == g_tuned.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+static void tuned_store(int kind, unsigned log2, const lsb_tuning& t) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[{kind, log2}] = t;
+}
+
+// Sweep of the fused path's launch shape on a sample batch (see lsb.h).
+template <class Tr>
+int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::Key* keys,
+             const uint64_t* vals, void* out, uint32_t out_kind, size_t n, cudaStream_t s,
+             lsb_tuning* best) {
+  lsb_tuning cur;
+  tb.get_tuning(&cur);
+  cudaEvent_t e0, e1;
+  LSB_CK(cudaEventCreate(&e0));
+  LSB_CK(cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  lsb_tuning win = cur;
+  int err = LSB_OK;
+  for (uint32_t block : {256u, 512u, 1024u}) {
+    for (uint32_t prefetch : {0u, 1u, 2u}) {
+      for (uint32_t chunk : {0u, 1024u, 2048u, 4096u}) {
+        lsb_tuning c = cur;
+        c.block_threads = block;
+        c.prefetch = prefetch;
+        c.chunk = chunk;
+        if (tb.set_tuning(c) != LSB_OK) continue;
+        if (tb.fused_grid() <= 0) continue;  // shape cannot be co-resident
+        err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);  // warm-up
+        if (err) break;
+        cudaEventRecord(e0, s);
+        err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);
+        cudaEventRecord(e1, s);
+        if (err) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+          err = LSB_ERR_CUDA;
+          break;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+          best_ms = ms;
+          win = c;
+        }
+      }
+      if (err) break;
+    }
+    if (err) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  tb.set_tuning(err ? cur : win);
+  if (err) return err;
+  tuned_store(kind, tb.log2, win);
+  if (best) *best = win;
+  return LSB_OK;
+}
+
+// A captured fused launch.
+struct lsb_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+template <class Tr>
+int capture_fused(Table<Tr>& tb, const uint8_t* types, const typename Tr::Key* keys,
+                  const uint64_t* vals, void* out, uint32_t out_kind, size_t n,
+                  lsb_graph** result) {
+  cudaStream_t cs;
+  LSB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  lsb_graph* g = new (std::nothrow) lsb_graph();
+  if (!g) {
+    cudaStreamDestroy(cs);
+    return LSB_ERR_OOM;
+  }
+  int err = LSB_OK;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    err = LSB_ERR_CUDA;
+  } else {
+    err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, cs);
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamEndCapture(cs, &graph) != cudaSuccess || graph == nullptr) {
+      if (!err) err = LSB_ERR_CUDA;
+    } else {
+      g->graph = graph;
+      if (!err && cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) err = LSB_ERR_CUDA;
+    }
+  }
+  cudaStreamDestroy(cs);
+  if (err) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    cudaGetLastError();
+    return err;
+  }
+  *result = g;
+  return LSB_OK;
+}
+
 struct lsb_map {
   Table<MapTraits> t;
 };
@@ -622,6 +755,8 @@ int lsb_map_create_ex(unsigned log2_buckets, const lsb_options* opt, lsb_map** o
     delete m;
     return e;
   }
+  lsb_tuning cached;
+  if (tuned_lookup(0, log2_buckets, &cached)) m->t.set_tuning(cached);
   *out = m;
   return LSB_OK;
 }
@@ -742,6 +877,8 @@ int lsb_set_create_ex(unsigned log2_buckets, const lsb_options* opt, lsb_set** o
     delete p;
     return e;
   }
+  lsb_tuning cached;
+  if (tuned_lookup(1, log2_buckets, &cached)) p->t.set_tuning(cached);
   *out = p;
   return LSB_OK;
 }
@@ -837,6 +974,51 @@ int lsb_set_size(lsb_set* p, uint64_t* count, cudaStream_t s) {
 int lsb_set_dump(lsb_set* p, uint32_t* keys_out, size_t cap, uint64_t* count, cudaStream_t s) {
   if (!p || (cap && !keys_out)) return LSB_ERR_ARG;
   return p->t.dump(keys_out, nullptr, cap, count, s);
+}
+
+// ------------------------------------------------------- graphs / autotune
+int lsb_map_autotune(lsb_map* m, const uint8_t* types, const uint64_t* keys, const uint64_t* vals,
+                     lsb_result* out, size_t n, cudaStream_t s, lsb_tuning* best) {
+  if (!m || !n || !types || !keys) return LSB_ERR_ARG;
+  if (!aligned(keys, 8) || !aligned(vals, 8) || !aligned(out, 8)) return LSB_ERR_ARG;
+  return autotune(m->t, 0, types, keys, vals, out, kOutResult, n, s, best);
+}
+
+int lsb_set_autotune(lsb_set* p, const uint8_t* types, const uint32_t* keys, bool* out, size_t n,
+                     cudaStream_t s, lsb_tuning* best) {
+  if (!p || !n || !types || !keys || !aligned(keys, 4)) return LSB_ERR_ARG;
+  return autotune(p->t, 1, types, keys, nullptr, out, kOutBool, n, s, best);
+}
+
+int lsb_autotune_lookup(int container, unsigned log2_buckets, lsb_tuning* out) {
+  if (!out || (container != 0 && container != 1)) return LSB_ERR_ARG;
+  return tuned_lookup(container, log2_buckets, out) ? LSB_OK : LSB_ERR_STATE;
+}
+
+int lsb_map_capture_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys,
+                          const uint64_t* vals, lsb_result* out, size_t n, lsb_graph** graph) {
+  if (!m || !graph || !n || !types || !keys) return LSB_ERR_ARG;
+  if (!aligned(keys, 8) || !aligned(vals, 8) || !aligned(out, 8)) return LSB_ERR_ARG;
+  return capture_fused(m->t, types, keys, vals, out, kOutResult, n, graph);
+}
+
+int lsb_set_capture_fused(lsb_set* p, const uint8_t* types, const uint32_t* keys, bool* out,
+                          size_t n, lsb_graph** graph) {
+  if (!p || !graph || !n || !types || !keys || !aligned(keys, 4)) return LSB_ERR_ARG;
+  return capture_fused(p->t, types, keys, nullptr, out, kOutBool, n, graph);
+}
+
+int lsb_graph_launch(lsb_graph* g, cudaStream_t s) {
+  if (!g || !g->exec) return LSB_ERR_ARG;
+  return cudaGraphLaunch(g->exec, s) == cudaSuccess ? LSB_OK : LSB_ERR_CUDA;
+}
+
+int lsb_graph_destroy(lsb_graph* g) {
+  if (!g) return LSB_ERR_ARG;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return LSB_OK;
 }
 
 // ------------------------------------------------------------------ misc

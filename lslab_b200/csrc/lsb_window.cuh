@@ -395,6 +395,9 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
     return;
   }
   __shared__ uint32_t s_base, s_next;
+  // whole tiles per claim: a tile crossing into the next claim would be
+  // processed twice (and a mutation would join its group twice)
+  chunk = max(32u * P, chunk - chunk % (32u * P));
   for (;;) {
     if (threadIdx.x == 0) {
       s_base = begin + atomicAdd(cursor, chunk);

@@ -253,3 +253,22 @@ def test_empty_and_bad_arguments(cuda):
     with pytest.raises(LsbError):
         Map(0)  # zero log2 buckets
     assert m.buckets() == 16
+
+
+@pytest.mark.parametrize("block", [256, 1024])
+@pytest.mark.parametrize("prefetch", [0, 1, 2])
+@pytest.mark.parametrize("chunk", [0, 2048])
+def test_every_tuning_is_exact(cuda, block, prefetch, chunk):
+    """Launch tuning never changes results (fused and per-phase paths)."""
+    n, log2 = 40_000, 6
+    types, keys, vals = _mixed_case(71, n, key_space=1500)
+    want = OracleMap(log2).mixed(types, keys, vals)
+    for fused in (True, False):
+        m = Map(log2, max_window=8192)
+        m.set_tuning(block_threads=block, prefetch=prefetch, chunk=chunk)
+        out = results_buf(n)
+        (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
+        _sync()
+        got = results(out)
+        assert same_results(got, want), f"fused={fused}: " + first_mismatch(got, want)
+        assert m.status() == 0
