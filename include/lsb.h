@@ -45,6 +45,7 @@ extern "C" {
 #define LSB_STATUS_TIMEOUT 0x2u
 #define LSB_STATUS_CHAIN 0x4u   /* a chain walk hit its hop limit */
 #define LSB_STATUS_BARRIER 0x8u /* a grid barrier gave up          */
+#define LSB_STATUS_SCRATCH 0x10u /* window scratch read back out of range; access skipped */
 
 /* ---- op codes of mixed batches -------------------------------------- */
 #define LSB_OP_GET 0u

@@ -22,12 +22,13 @@ import ctypes as C
 
 from . import _lib
 from ._lib import (LOCK_FREE, LOCK_RW, LOCK_WRITER, OP_CONTAINS, OP_GET, OP_INSERT, OP_PUT,
-                   OP_REMOVE, STATUS_BARRIER, STATUS_CHAIN, STATUS_OOM, STATUS_TIMEOUT, LsbError)
+                   OP_REMOVE, STATUS_BARRIER, STATUS_CHAIN, STATUS_OOM, STATUS_SCRATCH, STATUS_TIMEOUT,
+                   LsbError)
 
 __all__ = [
     "Map", "Set", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_CONTAINS", "OP_INSERT",
     "LOCK_WRITER", "LOCK_FREE", "LOCK_RW", "STATUS_OOM", "STATUS_TIMEOUT", "STATUS_CHAIN",
-    "STATUS_BARRIER", "lib",
+    "STATUS_BARRIER", "STATUS_SCRATCH", "lib",
 ]
 
 lib = _lib.lib

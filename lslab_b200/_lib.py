@@ -23,6 +23,7 @@ STATUS_OOM = 0x1
 STATUS_TIMEOUT = 0x2
 STATUS_CHAIN = 0x4
 STATUS_BARRIER = 0x8
+STATUS_SCRATCH = 0x10
 
 OP_GET = 0
 OP_PUT = 1

@@ -50,10 +50,23 @@ __global__ void __launch_bounds__(1024, 1)
   phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
 }
 
+// Ordering of the window's big groups; when hot keys produced groups of
+// more than kSortSmall members, the grid (a cooperative launch) continues
+// with the huge_* steps between grid barriers.
 template <class Tr>
-__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w) {
+__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
   phase_sort_big<Tr>(sc, w, smem);
+  if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe kernel has ended
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  uint32_t seq = 0;
+  huge_hist<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_scan<Tr>(sc, w, smem);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_runs<Tr>(sc, w, smem, gtid, gthreads);
 }
 
 template <class Tr>
@@ -147,12 +160,22 @@ __global__ void __launch_bounds__(1024, 1)
     // skips below are grid-uniform
     const bool has_big = ld_cg_u32(&w.cnt->big_count) != 0;
     const bool has_mut = ld_cg_u32(&w.cnt->mut_count) != 0;
+    const bool has_huge = huge_groups(sc, w.cnt) != 0;
     if (has_big || split < w.n) {
       if (has_big) phase_sort_big<Tr>(sc, w, smem);
+      if (has_huge) huge_hist<Tr>(sc, w, warp, nwarps);
       if (split < w.n)  // small claims so blocks freed by the sort take more
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
                                   blockDim.x * P, job.dedup != 0, ProbeSel{split, w.n, false},
                                   split & ~31u, perm);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+    }
+    if (has_huge) {
+      huge_scan<Tr>(sc, w, smem);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+      huge_scatter<Tr>(sc, w, warp, nwarps);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+      huge_runs<Tr>(sc, w, smem, tid, nt);
       if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     }
     trace_mark(job.trace, tat, wi, 2);
@@ -271,7 +294,8 @@ struct Table {
   void release() {
     void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
-                    sc.cnt, sc.obin, sc.perm, trace, fused_epoch};
+                    sc.cnt, sc.obin, sc.perm, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
+                    trace, fused_epoch};
     for (void* p : ptrs) cudaFree(p);
   }
 
@@ -299,6 +323,8 @@ struct Table {
     sc.gmask = g - 1;
     sc.cmask = cg - 1;
     sc.max_window = window;
+    sc.hcap = window / (kSortSmall + 1) + 1;
+    sc.rcap = window / kRunUnit + sc.hcap;
     bool ok =
         cudaMalloc(&slabs, slab_bytes) == cudaSuccess &&
         cudaMalloc(&locks, sizeof(int32_t) * buckets) == cudaSuccess &&
@@ -318,12 +344,18 @@ struct Table {
         cudaMalloc(&sc.large, sizeof(uint32_t) * (window / (kWarpSort + 1) + 1)) == cudaSuccess &&
         cudaMalloc(&sc.obin, window) == cudaSuccess &&
         cudaMalloc(&sc.perm, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.hlist, sizeof(uint32_t) * sc.hcap) == cudaSuccess &&
+        cudaMalloc(&sc.hrec, sizeof(uint32_t) * 4 * sc.hcap) == cudaSuccess &&
+        cudaMalloc(&sc.hbins, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap) == cudaSuccess &&
+        cudaMalloc(&sc.hrun, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap) == cudaSuccess &&
+        cudaMalloc(&sc.runs, sizeof(uint32_t) * 4 * (size_t)sc.rcap) == cudaSuccess &&
         cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess &&
         cudaMalloc(&fused_epoch, sizeof(uint32_t)) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       return LSB_ERR_OOM;
     }
+    sc.status = status;
     LSB_CK(cudaMemset(slabs, 0, slab_bytes));
     LSB_CK(cudaMemset(locks, 0, sizeof(int32_t) * buckets));
     LSB_CK(cudaMemset(status, 0, sizeof(uint32_t)));
@@ -333,6 +365,7 @@ struct Table {
     LSB_CK(cudaMemcpy(pool, p.data(), sizeof(uint64_t) * p.size(), cudaMemcpyHostToDevice));
     LSB_CK(cudaMemset(sc.gtab, 0, sizeof(uint64_t) * g));
     LSB_CK(cudaMemset(sc.ctab, 0, sizeof(uint64_t) * cg));
+    LSB_CK(cudaMemset(sc.hbins, 0, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap));
     LSB_CK(cudaMemset(sc.cnt, 0, kCounterBytes));
     LSB_CK(cudaMemset(fused_epoch, 0, sizeof(uint32_t)));
     bar = reinterpret_cast<GridBarrier*>(sc.cnt + 2);
@@ -448,10 +481,25 @@ struct Table {
       int e = next_plain_epoch(s, &w.epoch);
       if (e) return e;
       w.cnt = &sc.cnt[0];
-      LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
+      // the window's counters and the grid barrier of the sort launch
+      LSB_CK(cudaMemsetAsync(sc.cnt, 0, 2 * sizeof(WinCounters) + sizeof(GridBarrier), s));
       const int grid = grid_for(m);
       launch_probe<true>(grid, w, s);
-      k_sort<Tr><<<num_sms, 256, kSortSmemBytes, s>>>(sc, w);
+      {
+        GridBarrier* b = bar;
+        void* args[] = {&sc, &w, &b};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(num_sms);
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = kSortSmemBytes;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_sort<Tr>, args));
+      }
       const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
       k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w);
       LSB_CK(cudaGetLastError());

@@ -21,7 +21,9 @@
 #pragma once
 
 #include <cstdint>
+#ifndef LSB_HOST_EMU
 #include <cuda_runtime.h>
+#endif
 
 namespace lsb {
 
@@ -33,6 +35,7 @@ enum : uint32_t {
   kStatusTimeout = 0x2u,
   kStatusChain = 0x4u,
   kStatusBarrier = 0x8u,
+  kStatusScratch = 0x10u,
 };
 
 enum : uint8_t { kOpRead = 0, kOpWrite = 1, kOpRemove = 2 };  // get/contains, put/insert, remove
@@ -64,6 +67,12 @@ __device__ __forceinline__ uint32_t fingerprint(uint64_t h) {
 }
 
 // ------------------------------------------------------------- memory ops
+#ifdef LSB_HOST_EMU
+// CPU tests compile this header for the host with a thread-per-lane
+// emulation of a block; it supplies these helpers (and sm_id) as plain
+// atomic loads and stores.
+#include "emu_mem_ops.h"
+#else
 // Table reads go to L2 (.cg / .relaxed.gpu): the persistent kernel reads
 // slabs that other SMs wrote earlier in the same launch, and L1 is not
 // coherent across SMs.
@@ -188,6 +197,19 @@ __device__ __forceinline__ void st_cg_v2u64(void* p, uint64_t a, uint64_t b) {
   asm volatile("st.global.cg.v2.u64 [%0], {%1,%2};" ::"l"(p), "l"(a), "l"(b) : "memory");
 }
 
+__device__ __forceinline__ uint32_t atom_add_release(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t smid;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  return smid;
+}
+#endif  // LSB_HOST_EMU
+
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bits) {
   atomicOr(status, bits);
 }
@@ -282,8 +304,7 @@ constexpr uint32_t kPoolChunkMax = 32;
 // (include/lslab/detail/device_allocator.h:63-70): here exhaustion returns 0
 // and raises kStatusOOM.
 __device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
-  uint32_t smid;
-  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  const uint32_t smid = sm_id();
   unsigned long long* range = (unsigned long long*)&t.pool[2 + (smid & (kPoolSlots - 1))];
   unsigned long long old = atomicAdd(range, 1ull);
   uint32_t cur = (uint32_t)old, end = (uint32_t)(old >> 32);
@@ -688,12 +709,6 @@ struct GridBarrier {
   uint32_t count;  // arrivals in this launch (zeroed before the launch)
   uint32_t pad;
 };
-
-__device__ __forceinline__ uint32_t atom_add_release(uint32_t* p, uint32_t v) {
-  uint32_t old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
-}
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status,
                                              uint32_t& seq) {

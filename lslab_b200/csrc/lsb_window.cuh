@@ -61,6 +61,10 @@ struct WinCounters {
   uint32_t large_count;    // groups with more than kWarpSort members
   uint32_t large_work;
   uint32_t late_cursor;    // next late read handed out in the fused sort pass
+  uint32_t huge_count;     // groups with more than kSortSmall members
+  uint32_t huge_work;
+  uint32_t run_count;      // runs of huge groups (each sorted by one block)
+  uint32_t run_work;
   uint32_t pad[3];
 };
 
@@ -74,6 +78,10 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->large_count = 0;
   c->large_work = 0;
   c->late_cursor = 0;
+  c->huge_count = 0;
+  c->huge_work = 0;
+  c->run_count = 0;
+  c->run_work = 0;
 }
 
 // Scratch owned by a table, sized for max_window ops.
@@ -97,6 +105,16 @@ struct Scratch {
   WinCounters* cnt; // two sets, used by alternate windows
   uint8_t* obin;    // per op: table region (binned probing)
   uint32_t* perm;   // probe position -> op index (binned probing)
+  // groups of more than kSortSmall members (hot keys), ordered over several
+  // grid steps by many blocks: see the huge_* phases
+  uint32_t* hlist;  // group slots, hcap entries
+  uint32_t* hrec;   // per huge group: seg offset, stored members, first run, runs
+  uint32_t* hbins;  // per huge group: kHugeBins range counts, then cursors
+  uint32_t* hrun;   // per huge group and range: its run
+  uint32_t* runs;   // per run: seg begin, seg end, info, 1 + largest member
+  uint32_t hcap;
+  uint32_t rcap;
+  uint32_t* status; // the table's device status word
 };
 
 enum : uint32_t { kOutNone = 0, kOutResult = 1, kOutOld = 2, kOutBool = 3 };
@@ -169,9 +187,13 @@ __device__ __forceinline__ void write_result(const Window<Tr>& w, uint32_t i, ui
 }
 
 __device__ __forceinline__ uint32_t lane_id() {
+#ifdef LSB_HOST_EMU
+  return threadIdx.x & 31u;
+#else
   uint32_t l;
   asm("mov.u32 %0, %%laneid;" : "=r"(l));
   return l;
+#endif
 }
 
 __device__ __forceinline__ uint32_t gslot_of(uint64_t h, uint32_t gmask) {
@@ -242,6 +264,10 @@ __device__ __forceinline__ void group_store(const Scratch& sc, const Window<Tr>&
     if (cs != 0xFFFFFFFFu) sc.cdat[(size_t)cs * kChunk + q % kChunk] = i;
     if (pos == kInline) sc.big[atomicAdd(&w.cnt->big_count, 1u)] = slot;
     if (pos == kWarpSort) sc.large[atomicAdd(&w.cnt->large_count, 1u)] = slot;
+    if (pos == kSortSmall) {
+      const uint32_t h = atomicAdd(&w.cnt->huge_count, 1u);
+      if (h < sc.hcap) sc.hlist[h] = slot;
+    }
   }
 }
 
@@ -588,64 +614,49 @@ __device__ void bitmap_sort(const Scratch& sc, const Window<Tr>& w, uint32_t c, 
   }
 }
 
-// A group of more than kWarpSort members, ordered by the whole block.  Up to
-// kSortSmall members are gathered into shared memory first (a warp per
-// storage unit: the inline part, then each 32-member chunk with one
-// chunk-table lookup), so the counting sort reads only shared memory.
+// A group of kWarpSort+1 .. kSortSmall members, ordered by the whole block.
+// The members are gathered into shared memory first (a warp per storage
+// unit: the inline part, then each 32-member chunk with one chunk-table
+// lookup), so the counting sort reads only shared memory.
 template <class Tr>
 __device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_t gslot,
                                  uint32_t c, uint32_t off, uint32_t* smem) {
   uint32_t* sorted = smem + kSortSmall;
   uint32_t* bits = sorted + kSortSmall;
   uint32_t* pre = bits + kSortChunkWords;
-  if (c <= kSortSmall) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const uint32_t nchunks = (c - kInline + kChunk - 1) / kChunk;  // <= kSortSmall / kChunk
-    // all chunk-table lookups in flight at once (one per thread), parked in
-    // the prefix area; then each warp copies its chunks, loads issued before
-    // any store so they overlap
-    for (uint32_t k = tid; k < nchunks; k += blockDim.x) pre[k] = chunk_find(sc, w.epoch, gslot, k);
-    if (tid < kInline) smem[tid] = ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + tid]);
-    for (uint32_t j = tid; j < c; j += blockDim.x) sorted[j] = 0xFFFFFFFFu;  // holes stay invalid
-    __syncthreads();
-    for (uint32_t k0 = warp; k0 < nchunks; k0 += 4 * nwarps) {
-      uint32_t v[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t k = k0 + q * nwarps;
-        const uint32_t j = kInline + k * kChunk + lane;
-        const uint32_t cs = k < nchunks ? pre[k] : 0xFFFFFFFFu;
-        v[q] = (j < c && cs != 0xFFFFFFFFu) ? ld_cg_u32(&sc.cdat[(size_t)cs * kChunk + lane])
-                                            : 0xFFFFFFFFu;
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t j = kInline + (k0 + q * nwarps) * kChunk + lane;
-        if (j < c) smem[j] = v[q];
-      }
-    }
-    __syncthreads();
-    bitmap_sort<Tr>(sc, w, c, off, bits, pre, [&](uint32_t j) { return smem[j]; }, sorted);
-    // every member's predecessor from the sorted list in shared memory (the
-    // bitmap pass ends with a __syncthreads)
-    for (uint32_t j = tid; j < c; j += blockDim.x) {
-      const uint32_t e = sorted[j];
-      const uint32_t pe = j ? sorted[j - 1] : 0xFFFFFFFFu;
-      const uint32_t p = pe < w.n ? pe + 1 : 0u;
-      if (e < w.n) sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
-    }
-    __syncthreads();
-    return;
-  }
-  bitmap_sort<Tr>(sc, w, c, off, bits, pre,
-                  [&](uint32_t j) { return member_at(sc, w.epoch, gslot, j); }, nullptr);
-  __threadfence_block();
+  if (c > kSortSmall) return;  // block-uniform; larger groups take the huge_* phases
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t nchunks = (c - kInline + kChunk - 1) / kChunk;  // <= kSortSmall / kChunk
+  // all chunk-table lookups in flight at once (one per thread), parked in
+  // the prefix area; then each warp copies its chunks, loads issued before
+  // any store so they overlap
+  for (uint32_t k = tid; k < nchunks; k += blockDim.x) pre[k] = chunk_find(sc, w.epoch, gslot, k);
+  if (tid < kInline) smem[tid] = ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + tid]);
+  for (uint32_t j = tid; j < c; j += blockDim.x) sorted[j] = 0xFFFFFFFFu;  // holes stay invalid
   __syncthreads();
-  // every member's predecessor; op indices read back from scratch are checked
-  // before use as addresses
-  for (uint32_t j = threadIdx.x; j < c; j += blockDim.x) {
-    const uint32_t e = ld_cg_u32(&sc.seg[off + j]);
-    const uint32_t pe = j ? ld_cg_u32(&sc.seg[off + j - 1]) : 0xFFFFFFFFu;
+  for (uint32_t k0 = warp; k0 < nchunks; k0 += 4 * nwarps) {
+    uint32_t v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t k = k0 + q * nwarps;
+      const uint32_t j = kInline + k * kChunk + lane;
+      const uint32_t cs = k < nchunks ? pre[k] : 0xFFFFFFFFu;
+      v[q] = (j < c && cs != 0xFFFFFFFFu) ? ld_cg_u32(&sc.cdat[(size_t)cs * kChunk + lane])
+                                          : 0xFFFFFFFFu;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t j = kInline + (k0 + q * nwarps) * kChunk + lane;
+      if (j < c) smem[j] = v[q];
+    }
+  }
+  __syncthreads();
+  bitmap_sort<Tr>(sc, w, c, off, bits, pre, [&](uint32_t j) { return smem[j]; }, sorted);
+  // every member's predecessor from the sorted list in shared memory (the
+  // bitmap pass ends with a __syncthreads)
+  for (uint32_t j = tid; j < c; j += blockDim.x) {
+    const uint32_t e = sorted[j];
+    const uint32_t pe = j ? sorted[j - 1] : 0xFFFFFFFFu;
     const uint32_t p = pe < w.n ? pe + 1 : 0u;
     if (e < w.n) sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
   }
@@ -704,6 +715,10 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
     if (job >= nlarge) break;
     const uint32_t gslot = ld_cg_u32(&sc.large[job]) & sc.gmask;
     const uint32_t c = min(g_count(ld_relaxed_u64(&sc.gtab[gslot])), w.n);
+    if (c > kSortSmall) {  // the huge_* phases order it (c is block-uniform)
+      __syncthreads();      // s_job is rewritten next round
+      continue;
+    }
     if (tid == 0) {
       s_off = atomicAdd(&w.cnt->seg_cursor, c);
       sc.goff[gslot] = s_off;
@@ -728,6 +743,239 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
     }
     off = __shfl_sync(0xFFFFFFFFu, off, 0);
     sort_group_warp<Tr>(sc, w, gslot, c, off);
+  }
+}
+
+// ------------------------------------------------------- huge groups (D')
+// A group of more than kSortSmall members (a hot key) is ordered by the
+// whole grid in four steps separated by grid barriers, so no block reads
+// back global data that it wrote itself in the same step:
+//   hist     every warp takes storage units (inline part / 32-member chunks)
+//            of every huge group and counts members per index range
+//            (kHugeBins equal ranges of [0, n); a range is at most kRunUnit
+//            indices wide for windows up to 2^23 ops);
+//   scan     a block per group: range offsets in seg, the group's runs (a run
+//            starts at the first range beginning at or after each multiple of
+//            kRunUnit; ranges hold at most kRunUnit members, so a run is
+//            never empty and holds fewer than 2 * kRunUnit = kSortSmall) and
+//            each range's run;
+//   scatter  every warp again: members to their range's next free seg
+//            position; each run's largest member by atomicMax;
+//   runs     a block per run: counting sort in shared memory, written back
+//            in place, then each member's predecessor (the previous run's
+//            largest member for the first one).
+constexpr uint32_t kHugeBins = 4096;
+constexpr uint32_t kRunUnit = 2048;
+static_assert(2 * kRunUnit == kSortSmall, "a run fits the shared-memory sort");
+constexpr uint32_t kRunFirst = 1u << 30, kRunLast = 1u << 31;
+
+__device__ __forceinline__ uint32_t huge_width(uint32_t n) {
+  return (n + kHugeBins - 1) / kHugeBins;  // <= kRunUnit for n <= 2^23
+}
+
+__device__ __forceinline__ uint32_t huge_groups(const Scratch& sc, const WinCounters* c) {
+  return min(ld_cg_u32(&c->huge_count), sc.hcap);
+}
+
+// Member `lane` of storage unit k of group gslot (unit 0: the inline part,
+// unit k >= 1: chunk k-1), or 0xFFFFFFFF.  Whole warp.
+template <class Tr>
+__device__ __forceinline__ uint32_t huge_member(const Scratch& sc, const Window<Tr>& w,
+                                                uint32_t gslot, uint32_t c, uint32_t k,
+                                                uint32_t lane) {
+  if (k == 0)
+    return lane < kInline ? ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + lane]) : 0xFFFFFFFFu;
+  uint32_t cs = 0xFFFFFFFFu;
+  if (lane == 0) cs = chunk_find(sc, w.epoch, gslot, k - 1);
+  cs = __shfl_sync(0xFFFFFFFFu, cs, 0);
+  const uint32_t j = kInline + (k - 1) * kChunk + lane;
+  return (j < c && cs != 0xFFFFFFFFu) ? ld_cg_u32(&sc.cdat[(size_t)cs * kChunk + lane])
+                                      : 0xFFFFFFFFu;
+}
+
+template <class Tr>
+__device__ __forceinline__ uint32_t huge_size(const Scratch& sc, const Window<Tr>& w,
+                                              uint32_t h, uint32_t* gslot) {
+  *gslot = ld_cg_u32(&sc.hlist[h]) & sc.gmask;
+  return min(g_count(ld_relaxed_u64(&sc.gtab[*gslot])), w.n);
+}
+
+// hist: every warp of the grid (gwarp of ngwarps).
+template <class Tr>
+__device__ void huge_hist(const Scratch& sc, const Window<Tr>& w, uint32_t gwarp,
+                          uint32_t ngwarps) {
+  const uint32_t H = huge_groups(sc, w.cnt), width = huge_width(w.n), lane = lane_id();
+  for (uint32_t h = 0; h < H; ++h) {
+    uint32_t gslot;
+    const uint32_t c = huge_size(sc, w, h, &gslot);
+    const uint32_t units = 1 + (c - kInline + kChunk - 1) / kChunk;
+    uint32_t* bins = sc.hbins + (size_t)h * kHugeBins;
+    for (uint32_t k = gwarp; k < units; k += ngwarps) {
+      const uint32_t x = huge_member(sc, w, gslot, c, k, lane);
+      const uint32_t b = x < w.n ? x / width : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+      if (b != 0xFFFFFFFFu && lane == (uint32_t)__ffs(peers) - 1)
+        atomicAdd(&bins[b], (uint32_t)__popc(peers));
+    }
+  }
+}
+
+// scan: blocks take groups.  `smem` holds kSortSmemBytes (kHugeBins words
+// are used).
+template <class Tr>
+__device__ void huge_scan(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
+  __shared__ uint32_t s_h, s_off, s_base, s_last, s_tmp[32];
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t H = huge_groups(sc, w.cnt);
+  const uint32_t per = (kHugeBins + nt - 1) / nt, b0 = tid * per;
+  for (;;) {
+    if (tid == 0) {
+      s_h = atomicAdd(&w.cnt->huge_work, 1u);
+      s_last = 0;
+    }
+    __syncthreads();
+    const uint32_t h = s_h;
+    if (h >= H) break;
+    uint32_t gslot;
+    const uint32_t c = huge_size(sc, w, h, &gslot);
+    uint32_t* bins = sc.hbins + (size_t)h * kHugeBins;
+    uint32_t* hrun = sc.hrun + (size_t)h * kHugeBins;
+    uint32_t local = 0;
+    for (uint32_t k = 0; k < per; ++k)
+      if (b0 + k < kHugeBins) {
+        smem[b0 + k] = ld_cg_u32(&bins[b0 + k]);
+        local += smem[b0 + k];
+      }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(local, s_tmp, &total);
+    total = min(total, c);
+    uint32_t last = 0;  // offset of the last non-empty range
+    for (uint32_t k = 0; k < per; ++k)
+      if (b0 + k < kHugeBins) {
+        const uint32_t n = smem[b0 + k];
+        smem[b0 + k] = run;  // exclusive prefix
+        if (n) last = run;
+        run += n;
+      }
+    if (last) atomicMax(&s_last, last);
+    __syncthreads();
+    // run r exists when some non-empty range starts at or after r * kRunUnit,
+    // so no run is empty (a range holds at most kRunUnit members)
+    const uint32_t nrun = total ? min(s_last, total - 1) / kRunUnit + 1 : 0u;
+    if (tid == 0) {
+      s_off = atomicAdd(&w.cnt->seg_cursor, c);
+      sc.goff[gslot] = s_off;
+      s_base = atomicAdd(&w.cnt->run_count, nrun);
+    }
+    __syncthreads();
+    const uint32_t off = s_off, base = s_base;
+    if (tid == 0) {
+      uint32_t* rec = sc.hrec + 4 * (size_t)h;
+      rec[0] = off;
+      rec[1] = total;
+      rec[2] = base;
+      rec[3] = nrun;
+      if (nrun && base + nrun - 1 < sc.rcap) sc.runs[4 * (size_t)(base + nrun - 1) + 1] = off + total;
+    }
+    // cursors and runs of the ranges; run r begins at the first range whose
+    // offset is >= r * kRunUnit (the virtual range kHugeBins sits at total)
+    for (uint32_t b = tid; b <= kHugeBins; b += nt) {
+      const uint32_t p = b < kHugeBins ? min(smem[b], total) : total;
+      if (b < kHugeBins) {
+        bins[b] = off + p;
+        hrun[b] = base + min(p / kRunUnit, nrun ? nrun - 1 : 0u);
+      }
+      const uint32_t r0 = b ? min(smem[b - 1], total) / kRunUnit + 1 : 0u;
+      for (uint32_t r = r0; r <= p / kRunUnit; ++r) {
+        if (r < nrun && base + r < sc.rcap) {
+          uint32_t* rr = sc.runs + 4 * (size_t)(base + r);
+          rr[0] = off + p;
+          rr[2] = h | (r == 0 ? kRunFirst : 0u) | (r + 1 == nrun ? kRunLast : 0u);
+          rr[3] = 0;
+        }
+        if (r >= 1 && r < nrun && base + r - 1 < sc.rcap)  // the last run ends at total
+          sc.runs[4 * (size_t)(base + r - 1) + 1] = off + p;
+      }
+    }
+    for (uint32_t j = total + tid; j < c; j += nt) sc.seg[off + j] = 0xFFFFFFFFu;
+    __syncthreads();
+  }
+}
+
+// scatter: every warp of the grid.
+template <class Tr>
+__device__ void huge_scatter(const Scratch& sc, const Window<Tr>& w, uint32_t gwarp,
+                             uint32_t ngwarps) {
+  const uint32_t H = huge_groups(sc, w.cnt), width = huge_width(w.n), lane = lane_id();
+  for (uint32_t h = 0; h < H; ++h) {
+    uint32_t gslot;
+    const uint32_t c = huge_size(sc, w, h, &gslot);
+    const uint32_t units = 1 + (c - kInline + kChunk - 1) / kChunk;
+    uint32_t* bins = sc.hbins + (size_t)h * kHugeBins;
+    const uint32_t* hrun = sc.hrun + (size_t)h * kHugeBins;
+    const uint32_t end =
+        ld_cg_u32(&sc.hrec[4 * (size_t)h]) + ld_cg_u32(&sc.hrec[4 * (size_t)h + 1]);
+    for (uint32_t k = gwarp; k < units; k += ngwarps) {
+      const uint32_t x = huge_member(sc, w, gslot, c, k, lane);
+      const uint32_t b = x < w.n ? x / width : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+      const uint32_t leader = (uint32_t)__ffs(peers) - 1;
+      uint32_t p0 = 0;
+      if (b != 0xFFFFFFFFu && lane == leader) p0 = atomicAdd(&bins[b], (uint32_t)__popc(peers));
+      p0 = __shfl_sync(0xFFFFFFFFu, p0, leader);
+      if (b == 0xFFFFFFFFu) continue;
+      const uint32_t p = p0 + __popc(peers & ((1u << lane) - 1u));
+      if (p < end && p < sc.max_window) {
+        sc.seg[p] = x;
+        const uint32_t r = ld_cg_u32(&hrun[b]);
+        if (r < sc.rcap) atomicMax(&sc.runs[4 * (size_t)r + 3], x + 1);
+      } else {
+        raise_status(sc.status, kStatusScratch);
+      }
+    }
+  }
+}
+
+// runs: blocks take runs; the range counters are cleared for the next
+// window on the way (the scatter was their last user).
+template <class Tr>
+__device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem, uint32_t gtid,
+                          uint32_t gthreads) {
+  __shared__ uint32_t s_r;
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t H = huge_groups(sc, w.cnt);
+  for (size_t i = gtid; i < (size_t)H * kHugeBins; i += gthreads) sc.hbins[i] = 0;
+  const uint32_t R = min(ld_cg_u32(&w.cnt->run_count), sc.rcap);
+  uint32_t* sorted = smem + kSortSmall;
+  uint32_t* bits = sorted + kSortSmall;
+  uint32_t* pre = bits + kSortChunkWords;
+  for (;;) {
+    if (tid == 0) s_r = atomicAdd(&w.cnt->run_work, 1u);
+    __syncthreads();
+    const uint32_t r = s_r;
+    if (r >= R) break;
+    const uint4 rec = ld_cg_v4(&sc.runs[4 * (size_t)r]);
+    const uint32_t s = rec.x, e = rec.y, info = rec.z;
+    uint32_t n = 0;
+    if (s <= e && e - s <= kSortSmall && e <= sc.max_window)
+      n = e - s;
+    else if (tid == 0)
+      raise_status(sc.status, kStatusScratch);
+    for (uint32_t j = tid; j < n; j += nt) {
+      smem[j] = ld_cg_u32(&sc.seg[s + j]);
+      sorted[j] = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    if (n) bitmap_sort<Tr>(sc, w, n, s, bits, pre, [&](uint32_t j) { return smem[j]; }, sorted);
+    uint32_t first_pred = 0xFFFFFFFFu;
+    if (!(info & kRunFirst) && r > 0) first_pred = ld_cg_u32(&sc.runs[4 * (size_t)(r - 1) + 3]) - 1u;
+    for (uint32_t j = tid; j < n; j += nt) {
+      const uint32_t x = sorted[j];
+      const uint32_t pe = j ? sorted[j - 1] : first_pred;
+      const bool last = (info & kRunLast) && j + 1 == n;
+      if (x < w.n) sc.pred[x] = (pe < w.n ? pe + 1 : 0u) | (last ? kPredLast : 0u);
+    }
+    __syncthreads();
   }
 }
 

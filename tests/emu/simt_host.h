@@ -1,0 +1,236 @@
+// Host emulation of the CUDA execution model, for CPU tests of the library's
+// device functions (test infrastructure; never linked into the library).
+//
+// Every thread of an emulated block is a std::thread.  __syncthreads is a
+// barrier over the block; a warp intrinsic is an exchange through a per-warp
+// buffer between two barriers over the warp's 32 threads, so every lane must
+// take part (the library only uses full-warp masks).  Shared-memory variables
+// become function statics, which is correct while one block runs at a time.
+// Atomics are GCC __atomic builtins on host memory.
+#pragma once
+
+#include <barrier>
+#include <cassert>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#define __host__
+#define __device__
+#define __global__
+#define __forceinline__ inline
+#define __noinline__
+#define __launch_bounds__(...)
+#define __shared__ static
+#define __align__(n) alignas(n)
+
+struct uint4 {
+  uint32_t x, y, z, w;
+};
+struct ulonglong2 {
+  unsigned long long x, y;
+};
+struct dim3 {
+  unsigned x = 1, y = 1, z = 1;
+};
+
+inline thread_local dim3 threadIdx, blockIdx;
+inline dim3 blockDim, gridDim;
+
+namespace emu {
+
+struct Block {
+  std::unique_ptr<std::barrier<>> bar;
+  std::vector<std::unique_ptr<std::barrier<>>> warp_bar;
+  std::vector<uint64_t> buf;  // 32 words per warp
+};
+
+inline thread_local Block* blk = nullptr;
+
+inline uint64_t* wbuf() { return &blk->buf[(threadIdx.x >> 5) * 32]; }
+inline void wsync() { blk->warp_bar[threadIdx.x >> 5]->arrive_and_wait(); }
+
+template <class T>
+inline uint64_t to64(T v) {
+  static_assert(sizeof(T) <= 8, "warp exchange of at most 8 bytes");
+  uint64_t r = 0;
+  std::memcpy(&r, &v, sizeof(T));
+  return r;
+}
+template <class T>
+inline T from64(uint64_t r) {
+  T v;
+  std::memcpy(&v, &r, sizeof(T));
+  return v;
+}
+
+// Runs f() on every thread of one block of `nthreads` (a multiple of 32).
+template <class F>
+void run_block(unsigned nthreads, unsigned block, unsigned nblocks, F&& f) {
+  assert(nthreads % 32 == 0 && nthreads <= 1024);
+  Block b;
+  b.bar = std::make_unique<std::barrier<>>(nthreads);
+  for (unsigned w = 0; w < nthreads / 32; ++w)
+    b.warp_bar.push_back(std::make_unique<std::barrier<>>(32));
+  b.buf.assign(nthreads, 0);
+  blockDim.x = nthreads;
+  gridDim.x = nblocks;
+  std::vector<std::thread> th;
+  th.reserve(nthreads);
+  for (unsigned t = 0; t < nthreads; ++t)
+    th.emplace_back([&, t] {
+      threadIdx.x = t;
+      blockIdx.x = block;
+      blk = &b;
+      f();
+    });
+  for (auto& x : th) x.join();
+}
+
+}  // namespace emu
+
+inline void __syncthreads() { emu::blk->bar->arrive_and_wait(); }
+inline void __threadfence() { __atomic_thread_fence(__ATOMIC_SEQ_CST); }
+inline void __threadfence_block() { __atomic_thread_fence(__ATOMIC_SEQ_CST); }
+inline void __nanosleep(unsigned) { std::this_thread::yield(); }
+
+template <class T>
+inline T __shfl_sync(unsigned mask, T v, int src) {
+  assert(mask == 0xFFFFFFFFu);
+  uint64_t* b = emu::wbuf();
+  b[threadIdx.x & 31] = emu::to64(v);
+  emu::wsync();
+  const T r = emu::from64<T>(b[src & 31]);
+  emu::wsync();
+  return r;
+}
+
+template <class T>
+inline T __shfl_up_sync(unsigned mask, T v, unsigned d) {
+  assert(mask == 0xFFFFFFFFu);
+  const unsigned lane = threadIdx.x & 31;
+  uint64_t* b = emu::wbuf();
+  b[lane] = emu::to64(v);
+  emu::wsync();
+  const T r = lane >= d ? emu::from64<T>(b[lane - d]) : v;
+  emu::wsync();
+  return r;
+}
+
+inline unsigned __ballot_sync(unsigned mask, int pred) {
+  assert(mask == 0xFFFFFFFFu);
+  uint64_t* b = emu::wbuf();
+  b[threadIdx.x & 31] = pred ? 1 : 0;
+  emu::wsync();
+  unsigned r = 0;
+  for (unsigned l = 0; l < 32; ++l) r |= (unsigned)(b[l] & 1) << l;
+  emu::wsync();
+  return r;
+}
+
+template <class T>
+inline unsigned __match_any_sync(unsigned mask, T v) {
+  assert(mask == 0xFFFFFFFFu);
+  uint64_t* b = emu::wbuf();
+  const uint64_t me = emu::to64(v);
+  b[threadIdx.x & 31] = me;
+  emu::wsync();
+  unsigned r = 0;
+  for (unsigned l = 0; l < 32; ++l) r |= (unsigned)(b[l] == me) << l;
+  emu::wsync();
+  return r;
+}
+
+namespace emu {
+template <class Op>
+inline unsigned reduce(unsigned mask, unsigned v, Op op) {
+  assert(mask == 0xFFFFFFFFu);
+  uint64_t* b = wbuf();
+  b[threadIdx.x & 31] = v;
+  wsync();
+  unsigned r = (unsigned)b[0];
+  for (unsigned l = 1; l < 32; ++l) r = op(r, (unsigned)b[l]);
+  wsync();
+  return r;
+}
+}  // namespace emu
+
+inline unsigned __reduce_min_sync(unsigned m, unsigned v) {
+  return emu::reduce(m, v, [](unsigned a, unsigned b) { return a < b ? a : b; });
+}
+inline unsigned __reduce_max_sync(unsigned m, unsigned v) {
+  return emu::reduce(m, v, [](unsigned a, unsigned b) { return a > b ? a : b; });
+}
+inline unsigned __reduce_add_sync(unsigned m, unsigned v) {
+  return emu::reduce(m, v, [](unsigned a, unsigned b) { return a + b; });
+}
+
+inline int __popc(unsigned x) { return __builtin_popcount(x); }
+inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
+inline int __ffs(int x) { return __builtin_ffs(x); }
+inline unsigned __vcmpeq4(unsigned a, unsigned b) {
+  unsigned r = 0;
+  for (int i = 0; i < 4; ++i)
+    if (((a >> (8 * i)) & 0xFF) == ((b >> (8 * i)) & 0xFF)) r |= 0xFFu << (8 * i);
+  return r;
+}
+template <class T>
+inline T min(T a, T b) {
+  return a < b ? a : b;
+}
+template <class T>
+inline T max(T a, T b) {
+  return a > b ? a : b;
+}
+
+// The value operand converts to the pointee type, as CUDA's overloads do.
+template <class T, class U>
+inline T atomicAdd(T* p, U v) {
+  return __atomic_fetch_add(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U>
+inline T atomicSub(T* p, U v) {
+  return __atomic_fetch_sub(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U>
+inline T atomicAnd(T* p, U v) {
+  return __atomic_fetch_and(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U>
+inline T atomicOr(T* p, U v) {
+  return __atomic_fetch_or(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U>
+inline T atomicXor(T* p, U v) {
+  return __atomic_fetch_xor(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U>
+inline T atomicExch(T* p, U v) {
+  return __atomic_exchange_n(p, (T)v, __ATOMIC_SEQ_CST);
+}
+template <class T, class U, class V>
+inline T atomicCAS(T* p, U cmp_in, V v) {
+  T cmp = (T)cmp_in;
+  __atomic_compare_exchange_n(p, &cmp, (T)v, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+  return cmp;
+}
+template <class T, class U>
+inline T atomicMin(T* p, U v_in) {
+  const T v = (T)v_in;
+  T cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+  while (v < cur && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST,
+                                                 __ATOMIC_SEQ_CST)) {
+  }
+  return cur;
+}
+template <class T, class U>
+inline T atomicMax(T* p, U v_in) {
+  const T v = (T)v_in;
+  T cur = __atomic_load_n(p, __ATOMIC_SEQ_CST);
+  while (v > cur && !__atomic_compare_exchange_n(p, &cur, v, false, __ATOMIC_SEQ_CST,
+                                                 __ATOMIC_SEQ_CST)) {
+  }
+  return cur;
+}

@@ -1,0 +1,110 @@
+// CPU test driver for a whole map batch on the per-phase path (test
+// infrastructure): the library's probe, ordering and resolve phases run
+// window by window on an emulated grid with the launch shapes the library
+// uses (blocks of one step run one after another; no step waits on another
+// block).  Built with AddressSanitizer it checks every access of those
+// phases against its buffer; the results are written for comparison with
+// the oracle.
+//
+// usage: window_emu <ops file> <log2 buckets> <pool slabs> <block threads> <out file>
+// ops file: u32 n, u32 max_window, n x u8 type, n x u64 key, n x u64 value
+// out file: n x lsb_result (u8 found, 7 pad, u64 value), then u32 status
+#include "simt_host.h"
+#include "lsb_window.cuh"
+#include "emu_phases.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <vector>
+
+using namespace lsb;
+using Tr = MapTraits;
+
+int main(int argc, char** argv) {
+  if (argc != 6) {
+    std::fprintf(stderr, "usage: window_emu <ops> <log2> <pool> <block> <out>\n");
+    return 2;
+  }
+  FILE* f = std::fopen(argv[1], "rb");
+  if (!f) return 2;
+  uint32_t n = 0, window = 0;
+  if (std::fread(&n, 4, 1, f) != 1 || std::fread(&window, 4, 1, f) != 1) return 2;
+  std::vector<std::unique_ptr<uint8_t[]>> keep;
+  auto alloc = [&](size_t bytes) {
+    keep.emplace_back(new uint8_t[bytes]());
+    return (void*)keep.back().get();
+  };
+  uint8_t* types = (uint8_t*)alloc(n);
+  uint64_t* keys = (uint64_t*)alloc(8ull * n);
+  uint64_t* vals = (uint64_t*)alloc(8ull * n);
+  if (std::fread(types, 1, n, f) != n || std::fread(keys, 8, n, f) != n ||
+      std::fread(vals, 8, n, f) != n)
+    return 2;
+  std::fclose(f);
+  const unsigned log2 = (unsigned)std::atoi(argv[2]);
+  const uint64_t pool_slabs = std::strtoull(argv[3], nullptr, 10);
+  const unsigned block = (unsigned)std::atoi(argv[4]);
+  const uint32_t buckets = 1u << log2;
+  const unsigned num_sms = 148;
+
+  TableView t{};
+  t.slabs = (uint8_t*)alloc(((size_t)buckets + pool_slabs) * Tr::kSlabBytes);
+  t.locks = (int32_t*)alloc(4ull * buckets);
+  t.status = (uint32_t*)alloc(4);
+  t.pool = (uint64_t*)alloc(8ull * (2 + kPoolSlots));
+  t.pool[0] = buckets;
+  t.pool[1] = buckets + pool_slabs;
+  t.mask = buckets - 1;
+  t.lock_mode = kLockWriter;
+  t.chunk = (uint32_t)std::min<uint64_t>(kPoolChunkMax,
+                                         std::max<uint64_t>(1, pool_slabs / (8ull * num_sms)));
+  Scratch sc;
+  emu::alloc_scratch(sc, window, t.status, keep);
+  uint8_t* out = (uint8_t*)alloc(16ull * n);
+  std::vector<uint32_t> smem(kSortSmemBytes / 4);
+
+  uint32_t epoch = 0;
+  for (uint32_t off = 0; off < n; off += window) {
+    const uint32_t m = std::min(window, n - off);
+    Window<Tr> w{};
+    w.types = types + off;
+    w.keys = keys + off;
+    w.vals = vals + off;
+    w.out = out + (size_t)off * 16;
+    w.kstride = 1;
+    w.vstride = 1;
+    w.n = m;
+    epoch += 2;
+    w.epoch = epoch;
+    w.out_kind = kOutResult;
+    w.cnt = &sc.cnt[0];
+    std::memset(sc.cnt, 0, 2 * sizeof(WinCounters));
+    // probe: the library's grid for prefetch 0, static stride
+    const unsigned per_sm = 2048 / block;
+    const unsigned grid = std::max(1u, std::min(per_sm * num_sms, (m + block - 1) / block));
+    for (unsigned b = 0; b < grid; ++b)
+      emu::run_block(block, b, grid, [&] {
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+        phase_probe<Tr, true, 1>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, 0, false);
+      });
+    emu::sort_window<Tr>(sc, w, num_sms, 256, smem);
+    const unsigned rgrid = std::max(1u, std::min(num_sms * 8, (m + 255) / 256));
+    for (unsigned b = 0; b < rgrid; ++b)
+      emu::run_block(256, b, rgrid, [&] {
+        const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+        const uint32_t nt = gridDim.x * blockDim.x;
+        phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
+        phase_resolve_reads<Tr>(sc, w, tid, nt);
+      });
+  }
+  FILE* o = std::fopen(argv[5], "wb");
+  if (!o) return 2;
+  std::fwrite(out, 16, n, o);
+  std::fwrite(t.status, 4, 1, o);
+  std::fclose(o);
+  std::printf("done status=%#x\n", *t.status);
+  return 0;
+}

@@ -1,0 +1,116 @@
+"""CPU checks of the library's own device code under a host emulation of the
+CUDA execution model (tests/emu/simt_host.h): each CUDA thread is a host
+thread, each grid step runs all of its blocks before the next.
+
+The window-ordering phase (group formation, per-group ordering including the
+multi-step path for groups of more than 4096 members) is checked against the
+index order it must produce; the whole per-phase batch (probe, ordering,
+resolve) is built with AddressSanitizer, so every access of those phases is
+checked against its buffer, and its results are compared with the oracle."""
+from __future__ import annotations
+
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from lslab_b200 import workload as W
+from oracle import OracleMap
+
+ROOT = Path(__file__).resolve().parents[1]
+EMU = ROOT / "tests" / "emu"
+CSRC = ROOT / "lslab_b200" / "csrc"
+
+pytestmark = pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+
+
+def _build(out: Path, src: str, sanitize: bool) -> Path:
+    cmd = ["g++", "-std=c++20", "-O1", "-g", "-pthread", "-DLSB_HOST_EMU", f"-I{EMU}",
+           f"-I{CSRC}", str(EMU / src), "-o", str(out)]
+    if sanitize:
+        cmd[1:1] = ["-fsanitize=address", "-fno-omit-frame-pointer"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return out
+
+
+@pytest.fixture(scope="module")
+def bins(tmp_path_factory):
+    d = tmp_path_factory.mktemp("emu")
+    return {"order": _build(d / "order_emu", "order_emu.cpp", False),
+            "window": _build(d / "window_emu", "window_emu.cpp", True)}
+
+
+def _write_window(path: Path, types, keys, window, vals=None):
+    with open(path, "wb") as f:
+        f.write(np.array([len(keys), window], np.uint32).tobytes())
+        f.write(np.asarray(types, np.uint8).tobytes())
+        f.write(np.asarray(keys, np.uint64).tobytes())
+        if vals is not None:
+            f.write(np.asarray(vals, np.uint64).tobytes())
+
+
+def _order_cases():
+    rng = np.random.default_rng(5)
+    out = {}
+    n = 60_000  # one key carries half the ops: ~12k mutations in one group
+    t = rng.choice([0, 1, 2], size=n, p=[0.6, 0.3, 0.1]).astype(np.uint8)
+    k = W.key_of_rank(9, rng.integers(0, 40, size=n))
+    k[rng.random(n) < 0.5] = np.uint64(0xDEADBEEF)
+    out["hot"] = (t, k, 1 << 17)
+    n = 20_000  # every op a put of one key
+    out["one_key"] = (np.ones(n, np.uint8), np.full(n, 42, np.uint64), 1 << 15)
+    n = 10_001  # exactly 4097 members, window not a multiple of the range count
+    t = np.zeros(n, np.uint8)
+    k = W.key_of_rank(1, np.arange(n) % 97)
+    idx = np.sort(rng.choice(n, 4097, replace=False))
+    t[idx], k[idx] = 1, 5
+    out["just_over"] = (t, k, n)
+    n = 1 << 16  # a dense block of one key, a few strays far away, two more hot keys
+    t = rng.choice([0, 1, 2], size=n, p=[0.3, 0.5, 0.2]).astype(np.uint8)
+    k = W.key_of_rank(3, rng.integers(0, 3000, size=n))
+    k[30_000:40_000] = 8
+    k[rng.integers(0, n, size=20)] = 8
+    k[rng.random(n) < 0.15] = 9
+    k[rng.random(n) < 0.1] = 10
+    out["dense_and_strays"] = (t, k, 1 << 16)
+    return out
+
+
+ORDER = _order_cases()
+
+
+@pytest.mark.parametrize("case", sorted(ORDER))
+@pytest.mark.parametrize("threads,blocks", [(256, 3), (512, 2)])
+def test_ordering_matches_index_order(bins, tmp_path, case, threads, blocks):
+    t, k, window = ORDER[case]
+    path = tmp_path / "w.bin"
+    _write_window(path, t, k, window)
+    r = subprocess.run([str(bins["order"]), str(path), str(threads), str(blocks), "7"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.startswith("OK"), r.stdout + r.stderr
+
+
+def test_whole_batch_in_bounds_and_equal_to_oracle(bins, tmp_path):
+    """Probe, ordering (with a group of ~5k mutations) and resolve of a mixed
+    batch over two windows, under AddressSanitizer."""
+    n, log2 = 24_000, 6
+    rng = np.random.default_rng(11)
+    t = rng.choice([0, 1, 2], size=n, p=[0.5, 0.35, 0.15]).astype(np.uint8)
+    k = W.key_of_rank(2, rng.integers(0, 400, size=n))
+    k[rng.random(n) < 0.45] = np.uint64(77)
+    v = W.splitmix64(13, 0, n)
+    path, outp = tmp_path / "ops.bin", tmp_path / "out.bin"
+    _write_window(path, t, k, 16_384, v)
+    want = OracleMap(log2).mixed(t, k, v)
+    pool = (1 << log2) // 4 + 4096
+    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp)],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr[-4000:]
+    raw = np.fromfile(outp, np.uint8)
+    got = raw[: 16 * n].view(np.dtype([("found", "u1"), ("pad", "u1", (7,)), ("value", "<u8")]))
+    status = int(raw[16 * n:].view(np.uint32)[0])
+    assert status == 0
+    bad = np.nonzero((got["found"] != want["found"]) | (got["value"] != want["value"]))[0]
+    assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}"
