@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="zipf9505", choices=["zipf9505", "batches"],
+                    help="zipf9505: the headline line; batches: 4096 uneven mixed batches in "
+                         "one graph-captured fused launch vs per-op-type calls")
+    ap.add_argument("--nbatches", type=int, default=4096)
     ap.add_argument("--buckets-log2", type=int, default=22)
     ap.add_argument("--prefill-log2", type=int, default=26)
     ap.add_argument("--batch-log2", type=int, default=20)
@@ -569,11 +573,116 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_batches(args, world, rank, local):
+    """4096 mixed get/put/remove batches (lognormal sizes, median 512, sigma
+    1.5, clipped to [1, 2^18]; 80/15/5; Zipf 0.99 over 2^27 keys) on a map with
+    2^24 buckets prefilled with the 2^26 most popular keys.  Fused: the whole
+    batch stream as one autotuned, CUDA-graph-captured persistent launch.
+    Plain: per batch, one call per op type (get, put, remove), as the
+    reference's API issues them.  Results and final contents checked equal."""
+    import torch
+    import lslab_b200 as L
+    from lslab_b200 import workload as W
+    from lslab_b200.shard import rank_seed
+
+    seed = rank_seed(args.seed, rank)
+    log2, items, pre = 24, 1 << 27, 1 << 26
+    sizes = W.lognormal_sizes(seed, args.nbatches, 512, 1.5, 1, 1 << 18)
+    parts = [W.map_zipf_batch(seed, b, int(n), items, 0.99, (0.8, 0.15, 0.05))
+             for b, n in enumerate(sizes)]
+    types = np.concatenate([p.types for p in parts])
+    keys = np.concatenate([p.keys for p in parts])
+    vals = np.concatenate([p.vals for p in parts])
+    n = len(keys)
+    pk = W.key_of_rank(seed, np.arange(pre))
+    fused = L.Map(log2, 1 << 22)
+    plain = L.Map(log2, 1 << 22)
+    for off in range(0, pre, 1 << 24):
+        k = dev_u64(torch, pk[off:off + (1 << 24)])
+        fused.put(k, k)
+        plain.put(k, k)
+        del k
+    d_types = torch.from_numpy(types).cuda()
+    d_keys, d_vals = dev_u64(torch, keys), dev_u64(torch, vals)
+    out_f = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    # autotune on a sample (the first 256 batches); the plain table gets the
+    # sample once as well, so both tables stay identical
+    ns = int(sum(sizes[:256]))
+    tuned = fused.autotune(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
+    plain.execute(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
+    graph = fused.capture_fused(d_types, d_keys, d_vals, out_f)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    cnt = [(int(np.sum(p.types == 0)), int(np.sum(p.types == 1))) for p in parts]
+    d_out_g = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    d_out_p = torch.empty(n, dtype=torch.int64, device="cuda")
+
+    def plain_pass():
+        for b, (g, p) in enumerate(cnt):
+            o = int(offs[b])
+            r = int(sizes[b]) - g - p
+            if g:
+                plain.get(d_keys[o:o + g], d_out_g[o:o + g])
+            if p:
+                plain.put(d_keys[o + g:o + g + p], d_vals[o + g:o + g + p], d_out_p[o + g:o + g + p])
+            if r:
+                plain.remove(d_keys[o + g + p:o + g + p + r], d_out_g[o + g + p:o + g + p + r])
+
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    reps = max(1, args.steps)
+    f_ms, p_ms, identical = [], [], True
+    for rep in range(reps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        graph.launch()
+        e[1].record(stream)
+        e[2].record(stream)
+        plain_pass()
+        e[3].record(stream)
+        torch.cuda.synchronize()
+        f_ms.append(e[0].elapsed_time(e[1]))
+        p_ms.append(e[2].elapsed_time(e[3]))
+        if rep == 0:
+            # fused results vs the per-type calls of the same batches
+            isput = torch.from_numpy(types == 1).cuda()
+            got_f = out_f.clone()
+            want = d_out_g.clone()
+            want[isput, 0] = -1  # put results compared on the value only
+            got_f[isput, 0] = -1
+            want[isput, 1] = d_out_p[isput]
+            identical = bool(torch.equal(got_f, want))
+    kf, vf = fused.dump()
+    kp, vp = plain.dump()
+    identical = identical and np.array_equal(kf, kp) and np.array_equal(vf, vp)
+    graph.close()
+    fm, pm = statistics.median(f_ms), statistics.median(p_ms)
+    line = {
+        "workload": "batches",
+        "description": (f"{args.nbatches} mixed batches (lognormal median 512, sigma 1.5), "
+                        f"80/15/5 get/put/remove, Zipf 0.99 over 2^27 keys, map 2^24 "
+                        f"buckets prefilled with 2^26 keys"),
+        "ops": n, "batches": args.nbatches, "reps": reps,
+        "fused_mops": round(n / (fm * 1e-3) / 1e6, 1),
+        "plain_mops": round(n / (pm * 1e-3) / 1e6, 1),
+        "fused_over_plain": round(pm / fm, 2),
+        "fused_ms": [round(x, 3) for x in f_ms], "plain_ms": [round(x, 2) for x in p_ms],
+        "results_identical": identical, "tuning": tuned,
+        "plain_calls_per_pass": int(sum((g > 0) + (p > 0) + (int(sizes[b]) - g - p > 0)
+                                        for b, (g, p) in enumerate(cnt))),
+        "fused_launches_per_pass": 1,
+        "device_status": fused.status() | plain.status(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank, local)
+    elif args.workload == "batches":
+        run_batches(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
     if world > 1:

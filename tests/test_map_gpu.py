@@ -119,6 +119,35 @@ def test_hot_key_big_groups(cuda, fused):
     assert m.status() == 0
 
 
+@pytest.mark.parametrize("fused", [False, True])
+def test_huge_skewed_groups(cuda, fused):
+    """Groups far above the shared-memory sort size in one 2^20-op window:
+    one key spread over the whole window, one packed densely into a narrow
+    index range with a few strays far away (a very uneven spread of member
+    indices), and a dozen Zipf-hot keys."""
+    n = 1 << 20
+    rng = np.random.default_rng(17)
+    types = rng.choice([OP_GET, OP_PUT, OP_REMOVE], size=n, p=[0.5, 0.35, 0.15]).astype(np.uint8)
+    keys = W.key_of_rank(4, rng.zipf(1.3, size=n).astype(np.uint64) % np.uint64(5000))
+    keys[rng.random(n) < 0.2] = np.uint64(7)
+    dense = slice(600_000, 640_000)
+    keys[dense] = np.where(rng.random(40_000) < 0.8, np.uint64(8), keys[dense])
+    keys[rng.integers(0, n, size=50)] = np.uint64(8)
+    vals = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
+    o = OracleMap(10)
+    want = o.mixed(types, keys, vals)
+    m = Map(10, max_window=n)
+    out = results_buf(n)
+    (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)
+    assert m.status() == 0
+
+
 def test_type_sorted_batches_plain_equals_fused(cuda):
     """The 95/5 Zipf workload shape at small size: per-op-type calls (gets then
     puts) and the fused path give identical results, equal to the oracle."""
