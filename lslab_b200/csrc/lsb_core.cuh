@@ -197,9 +197,13 @@ __device__ __forceinline__ void st_cg_v2u64(void* p, uint64_t a, uint64_t b) {
   asm volatile("st.global.cg.v2.u64 [%0], {%1,%2};" ::"l"(p), "l"(a), "l"(b) : "memory");
 }
 
-__device__ __forceinline__ uint32_t atom_add_release(uint32_t* p, uint32_t v) {
+// Acquire-release: the block that arrives last at a grid barrier reads the
+// other blocks' arrivals with this add and then proceeds without polling, so
+// the add itself must acquire (a release-only add would let that block read
+// stale copies of data the others wrote before arriving).
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
   uint32_t old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
 
@@ -686,6 +690,11 @@ __device__ __forceinline__ void table_apply_known(const TableView& t, typename T
     if (present) table_apply<Tr>(t, key, h, true, val);
     return;
   }
+  // the location was read back from window scratch: check it before use
+  if (((loc & ~kLocLive) >> 8) >= ld_cg_u64(&t.pool[1]) || loc_slot(loc) >= kSlots) {
+    raise_status(t.status, kStatusScratch);
+    return;
+  }
   uint8_t* slab = slab_ptr(t.slabs, loc_slab(loc), Tr::kSlabBytes);
   const int slot = loc_slot(loc);
   if (present) {
@@ -700,8 +709,8 @@ __device__ __forceinline__ void table_apply_known(const TableView& t, typename T
 // -------------------------------------------------------- grid barrier
 // Monotonic-count barrier for a cooperative (co-resident) grid: barrier k of
 // a launch completes when the arrival counter reaches (k + 1) * nblocks, so
-// nothing is reset between barriers.  One thread per block arrives with a
-// release add and polls with acquire loads; the block's other threads are
+// nothing is reset between barriers.  One thread per block arrives with an
+// acquire-release add and polls with acquire loads; the block's other threads are
 // ordered by __syncthreads on both sides.  Each wait polls at most
 // kBarrierPolls times; on timeout it raises kStatusBarrier and returns false
 // so the caller can leave the kernel.
@@ -718,7 +727,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, u
   if (threadIdx.x == 0) {
     ok = 1;
     const uint32_t target = seq * nblocks;
-    if (atom_add_release(&b->count, 1u) + 1 != target) {
+    if (atom_add_acq_rel(&b->count, 1u) + 1 != target) {
       uint32_t it = 0;
       while ((int32_t)(ld_acquire_u32(&b->count) - target) < 0) {
         if (++it > kBarrierPolls || (*(volatile uint32_t*)status & kStatusBarrier)) {

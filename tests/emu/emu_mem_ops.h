@@ -45,7 +45,7 @@ inline void st_cg_v2u64(void* p, uint64_t a, uint64_t b) {
   emu_detail::st<uint64_t>(p, a);
   emu_detail::st<uint64_t>(static_cast<uint64_t*>(p) + 1, b);
 }
-inline uint32_t atom_add_release(uint32_t* p, uint32_t v) {
-  return __atomic_fetch_add(p, v, __ATOMIC_RELEASE);
+inline uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+  return __atomic_fetch_add(p, v, __ATOMIC_ACQ_REL);
 }
 inline uint32_t sm_id() { return blockIdx.x; }
