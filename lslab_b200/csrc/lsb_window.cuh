@@ -62,10 +62,8 @@ struct WinCounters {
   uint32_t large_work;
   uint32_t late_cursor;    // next late read handed out in the fused sort pass
   uint32_t huge_count;     // groups with more than kSortSmall members
-  uint32_t huge_work;
   uint32_t run_count;      // runs of huge groups (each sorted by one block)
-  uint32_t run_work;
-  uint32_t pad[3];
+  uint32_t pad[5];
 };
 
 __device__ inline void win_counters_reset(WinCounters* c) {
@@ -79,9 +77,7 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->large_work = 0;
   c->late_cursor = 0;
   c->huge_count = 0;
-  c->huge_work = 0;
   c->run_count = 0;
-  c->run_work = 0;
 }
 
 // Scratch owned by a table, sized for max_window ops.
@@ -820,22 +816,18 @@ __device__ void huge_hist(const Scratch& sc, const Window<Tr>& w, uint32_t gwarp
   }
 }
 
-// scan: blocks take groups.  `smem` holds kSortSmemBytes (kHugeBins words
-// are used).
+// scan: block b takes groups b, b + gridDim.x, ... (every thread derives the
+// group itself: no claim is broadcast through shared memory).  `smem` holds
+// kSortSmemBytes (kHugeBins words are used).
 template <class Tr>
 __device__ void huge_scan(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
-  __shared__ uint32_t s_h, s_off, s_base, s_last, s_tmp[32];
+  __shared__ uint32_t s_off, s_base, s_last, s_tmp[32];
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
   const uint32_t H = huge_groups(sc, w.cnt);
   const uint32_t per = (kHugeBins + nt - 1) / nt, b0 = tid * per;
-  for (;;) {
-    if (tid == 0) {
-      s_h = atomicAdd(&w.cnt->huge_work, 1u);
-      s_last = 0;
-    }
+  for (uint32_t h = blockIdx.x; h < H; h += gridDim.x) {
+    if (tid == 0) s_last = 0;
     __syncthreads();
-    const uint32_t h = s_h;
-    if (h >= H) break;
     uint32_t gslot;
     const uint32_t c = huge_size(sc, w, h, &gslot);
     uint32_t* bins = sc.hbins + (size_t)h * kHugeBins;
@@ -936,12 +928,11 @@ __device__ void huge_scatter(const Scratch& sc, const Window<Tr>& w, uint32_t gw
   }
 }
 
-// runs: blocks take runs; the range counters are cleared for the next
-// window on the way (the scatter was their last user).
+// runs: block b takes runs b, b + gridDim.x, ...; the range counters are
+// cleared for the next window on the way (the scatter was their last user).
 template <class Tr>
 __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem, uint32_t gtid,
                           uint32_t gthreads) {
-  __shared__ uint32_t s_r;
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
   const uint32_t H = huge_groups(sc, w.cnt);
   for (size_t i = gtid; i < (size_t)H * kHugeBins; i += gthreads) sc.hbins[i] = 0;
@@ -949,11 +940,7 @@ __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
   uint32_t* sorted = smem + kSortSmall;
   uint32_t* bits = sorted + kSortSmall;
   uint32_t* pre = bits + kSortChunkWords;
-  for (;;) {
-    if (tid == 0) s_r = atomicAdd(&w.cnt->run_work, 1u);
-    __syncthreads();
-    const uint32_t r = s_r;
-    if (r >= R) break;
+  for (uint32_t r = blockIdx.x; r < R; r += gridDim.x) {
     const uint4 rec = ld_cg_v4(&sc.runs[4 * (size_t)r]);
     const uint32_t s = rec.x, e = rec.y, info = rec.z;
     uint32_t n = 0;

@@ -98,10 +98,12 @@ def test_mixed_conflicts_vs_oracle(cuda, fused, window):
     assert m.status() == 0
 
 
-@pytest.mark.parametrize("fused", [False, True])
-def test_hot_key_big_groups(cuda, fused):
-    """One key carries thousands of mutations in one window (block-wide sort
-    path) interleaved with reads of it and of other keys."""
+@pytest.mark.parametrize("fused,block", [(False, 512), (True, 128), (True, 256), (True, 512),
+                                         (True, 1024)])
+def test_hot_key_big_groups(cuda, fused, block):
+    """One key carries ~40k mutations in one window (the multi-step ordering
+    of hot keys) and 50 keys ~800 each (block-wide ordering), interleaved
+    with reads of them; every launch shape of the fused kernel."""
     n = 200_000
     rng = np.random.default_rng(3)
     types = rng.choice([OP_GET, OP_PUT, OP_REMOVE], size=n, p=[0.6, 0.3, 0.1]).astype(np.uint8)
@@ -111,6 +113,7 @@ def test_hot_key_big_groups(cuda, fused):
     o = OracleMap(8)
     want = o.mixed(types, keys, vals)
     m = Map(8)
+    m.set_tuning(block_threads=block)
     out = results_buf(n)
     (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
     _sync()
