@@ -323,7 +323,7 @@ struct Table {
     sc.gmask = g - 1;
     sc.cmask = cg - 1;
     sc.max_window = window;
-    sc.hcap = window / (kSortSmall + 1) + 1;
+    sc.hcap = window / (kHugeMin + 1) + 1;
     sc.rcap = window / kRunUnit + sc.hcap;
     bool ok =
         cudaMalloc(&slabs, slab_bytes) == cudaSuccess &&

@@ -39,7 +39,10 @@ constexpr uint32_t kChunk = 32;        // members per overflow chunk
 constexpr uint32_t kPredLast = 0x80000000u;
 constexpr uint32_t kPredMask = 0x7FFFFFFFu;  // predecessor op index + 1; 0 = none
 constexpr uint32_t kWarpSort = 64;    // groups up to this size are ordered by one warp
-constexpr uint32_t kSortSmall = 4096;  // larger groups up to this size sort in shared memory
+constexpr uint32_t kSortSmall = 4096;  // members a shared-memory sort holds
+// groups of more than kHugeMin members are ordered by many blocks (the huge_*
+// steps); smaller big groups by one block or one warp
+constexpr uint32_t kHugeMin = 4096;
 constexpr uint32_t kSortChunkWords = 2048;  // bitmap words per counting-sort pass
 // shared memory of the sort: kSortSmall members + kSortSmall sorted + bitmap
 // + prefix words
@@ -55,13 +58,13 @@ struct WinCounters {
   uint32_t mut_count;
   uint32_t seg_cursor;
   uint32_t big_count;
-  uint32_t big_work;
+  uint32_t pad0;
   uint32_t inv_first_mut;  // ~(lowest mutation index); 0 = no mutation
   uint32_t probe_cursor;   // next op to hand out when the probe claims chunks
   uint32_t large_count;    // groups with more than kWarpSort members
-  uint32_t large_work;
+  uint32_t pad1;
   uint32_t late_cursor;    // next late read handed out in the fused sort pass
-  uint32_t huge_count;     // groups with more than kSortSmall members
+  uint32_t huge_count;     // groups with more than kHugeMin members
   uint32_t run_count;      // runs of huge groups (each sorted by one block)
   uint32_t pad[5];
 };
@@ -70,11 +73,9 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->mut_count = 0;
   c->seg_cursor = 0;
   c->big_count = 0;
-  c->big_work = 0;
   c->inv_first_mut = 0;
   c->probe_cursor = 0;
   c->large_count = 0;
-  c->large_work = 0;
   c->late_cursor = 0;
   c->huge_count = 0;
   c->run_count = 0;
@@ -101,7 +102,7 @@ struct Scratch {
   WinCounters* cnt; // two sets, used by alternate windows
   uint8_t* obin;    // per op: table region (binned probing)
   uint32_t* perm;   // probe position -> op index (binned probing)
-  // groups of more than kSortSmall members (hot keys), ordered over several
+  // groups of more than kHugeMin members (hot keys), ordered over several
   // grid steps by many blocks: see the huge_* phases
   uint32_t* hlist;  // group slots, hcap entries
   uint32_t* hrec;   // per huge group: seg offset, stored members, first run, runs
@@ -260,7 +261,7 @@ __device__ __forceinline__ void group_store(const Scratch& sc, const Window<Tr>&
     if (cs != 0xFFFFFFFFu) sc.cdat[(size_t)cs * kChunk + q % kChunk] = i;
     if (pos == kInline) sc.big[atomicAdd(&w.cnt->big_count, 1u)] = slot;
     if (pos == kWarpSort) sc.large[atomicAdd(&w.cnt->large_count, 1u)] = slot;
-    if (pos == kSortSmall) {
+    if (pos == kHugeMin) {
       const uint32_t h = atomicAdd(&w.cnt->huge_count, 1u);
       if (h < sc.hcap) sc.hlist[h] = slot;
     }
@@ -610,7 +611,7 @@ __device__ void bitmap_sort(const Scratch& sc, const Window<Tr>& w, uint32_t c, 
   }
 }
 
-// A group of kWarpSort+1 .. kSortSmall members, ordered by the whole block.
+// A group of kWarpSort+1 .. kHugeMin members, ordered by the whole block.
 // The members are gathered into shared memory first (a warp per storage
 // unit: the inline part, then each 32-member chunk with one chunk-table
 // lookup), so the counting sort reads only shared memory.
@@ -696,42 +697,37 @@ __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t
   }
 }
 
-// Phase D: blocks first take the large groups (the critical path), then each
-// warp takes the remaining groups of the big list.  `smem` holds
-// kSortSmemBytes.
+// Phase D: block b orders large groups b, b + gridDim.x, ... (the critical
+// path); then warps take the groups of the big list by a static stride that
+// starts at the warps of blocks without a large group.  No work is claimed
+// through a shared counter, so no grid-wide atomic serializes the phase.
+// `smem` holds kSortSmemBytes.
 template <class Tr>
 __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
-  __shared__ uint32_t s_job, s_off;
+  __shared__ uint32_t s_off;
   const uint32_t tid = threadIdx.x;
   const uint32_t nlarge = ld_cg_u32(&w.cnt->large_count);
-  for (;;) {
-    if (tid == 0) s_job = atomicAdd(&w.cnt->large_work, 1u);
-    __syncthreads();
-    const uint32_t job = s_job;
-    if (job >= nlarge) break;
+  for (uint32_t job = blockIdx.x; job < nlarge; job += gridDim.x) {
     const uint32_t gslot = ld_cg_u32(&sc.large[job]) & sc.gmask;
     const uint32_t c = min(g_count(ld_relaxed_u64(&sc.gtab[gslot])), w.n);
-    if (c > kSortSmall) {  // the huge_* phases order it (c is block-uniform)
-      __syncthreads();      // s_job is rewritten next round
-      continue;
-    }
+    if (c > kHugeMin) continue;  // the huge_* steps order it (c is block-uniform)
     if (tid == 0) {
       s_off = atomicAdd(&w.cnt->seg_cursor, c);
       sc.goff[gslot] = s_off;
     }
     __syncthreads();
-    sort_group_block<Tr>(sc, w, gslot, c, s_off, smem);
+    const uint32_t off = s_off;
+    sort_group_block<Tr>(sc, w, gslot, c, off, smem);  // ends with __syncthreads
   }
   const uint32_t nbig = ld_cg_u32(&w.cnt->big_count);
-  const uint32_t lane = lane_id();
-  for (;;) {
-    uint32_t job = 0;
-    if (lane == 0) job = atomicAdd(&w.cnt->big_work, 1u);
-    job = __shfl_sync(0xFFFFFFFFu, job, 0);
-    if (job >= nbig) break;
+  const uint32_t lane = lane_id(), wpb = blockDim.x >> 5;
+  const uint32_t nw = gridDim.x * wpb;
+  const uint32_t busy = min(nlarge, gridDim.x) * wpb;  // warps of blocks with a large group
+  const uint32_t gw = blockIdx.x * wpb + (threadIdx.x >> 5);
+  for (uint32_t job = (gw + nw - busy % nw) % nw; job < nbig; job += nw) {
     const uint32_t gslot = ld_cg_u32(&sc.big[job]) & sc.gmask;
     const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[gslot]));
-    if (c > kWarpSort) continue;  // a block took it
+    if (c > kWarpSort) continue;  // a block (or the huge steps) took it
     uint32_t off = 0;
     if (lane == 0) {
       off = atomicAdd(&w.cnt->seg_cursor, c);
@@ -743,7 +739,7 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
 }
 
 // ------------------------------------------------------- huge groups (D')
-// A group of more than kSortSmall members (a hot key) is ordered by the
+// A group of more than kHugeMin members (a hot key) is ordered by the
 // whole grid in four steps separated by grid barriers, so no block reads
 // back global data that it wrote itself in the same step:
 //   hist     every warp takes storage units (inline part / 32-member chunks)
