@@ -69,11 +69,15 @@ __global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, Grid
   huge_runs<Tr>(sc, w, smem, gtid, gthreads);
 }
 
+// Last kernel of a per-phase window: it also leaves the counter block zeroed
+// for the next launch.
 template <class Tr>
-__global__ void __launch_bounds__(1024, 1) k_resolve(TableView t, Scratch sc, Window<Tr> w) {
+__global__ void __launch_bounds__(1024, 1)
+    k_resolve(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
   phase_resolve_reads<Tr>(sc, w, tid, nt);
+  release_counters(sc.cnt, bar, nullptr, 0);
 }
 
 // One batch split into windows, all phases of all windows in one cooperative
@@ -102,9 +106,8 @@ __device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t 
 }
 
 template <class Tr, int P>
-__global__ void __launch_bounds__(1024, 1)
-    k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
-  extern __shared__ uint32_t smem[];
+__device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
+                              GridBarrier* bar, uint32_t* smem) {
   const uint32_t nblocks = gridDim.x;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   const uint32_t warp = tid >> 5, nwarps = nt >> 5;
@@ -189,6 +192,14 @@ __global__ void __launch_bounds__(1024, 1)
     if (wi + 1 < nwin && !grid_barrier(bar, nblocks, t.status, seq)) return;
     trace_mark(job.trace, tat, wi, 3);
   }
+}
+
+template <class Tr, int P>
+__global__ void __launch_bounds__(1024, 1)
+    k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
+  extern __shared__ uint32_t smem[];
+  fused_windows<Tr, P>(t, sc, job, bar, smem);
+  release_counters(sc.cnt, bar, job.bins, 2 * sizeof(BinCounters) / 4);
 }
 
 // Live-entry count and dump: one thread per bucket walks the chain.
@@ -460,8 +471,9 @@ struct Table {
       Window<Tr> w = window(nullptr, kOpRead, keys + off, 1, nullptr, 1,
                             out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr, out_kind, m);
       w.cnt = &sc.cnt[0];
-      if (tune.chunk) LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
       launch_probe<false>(grid_for(m), w, s);
+      // the probe's claim cursor is the only counter it uses: clear it again
+      if (tune.chunk) LSB_CK(cudaMemsetAsync(w.cnt, 0, sizeof(WinCounters), s));
       LSB_CK(cudaGetLastError());
     }
     return LSB_OK;
@@ -481,8 +493,8 @@ struct Table {
       int e = next_plain_epoch(s, &w.epoch);
       if (e) return e;
       w.cnt = &sc.cnt[0];
-      // the window's counters and the grid barrier of the sort launch
-      LSB_CK(cudaMemsetAsync(sc.cnt, 0, 2 * sizeof(WinCounters) + sizeof(GridBarrier), s));
+      // the counters and the sort launch's grid barrier are zero here: the
+      // previous launch's last block cleared them (release_counters)
       const int grid = grid_for(m);
       launch_probe<true>(grid, w, s);
       {
@@ -501,7 +513,7 @@ struct Table {
         LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_sort<Tr>, args));
       }
       const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
-      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w);
+      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar);
       LSB_CK(cudaGetLastError());
     }
     return LSB_OK;
@@ -541,8 +553,8 @@ struct Table {
     const int grid = fused_grid();
     if (grid <= 0) return LSB_ERR_STATE;
     job.fused_epoch = fused_epoch;
-    // counters of both windows, the barrier and the region counters: one memset
-    LSB_CK(cudaMemsetAsync(sc.cnt, 0, kCounterBytes, s));
+    // counters of both windows, the barrier and the region counters are zero
+    // here: the previous launch's last block cleared them (release_counters)
     TableView tv = view();
     Scratch scv = sc;
     GridBarrier* b = bar;

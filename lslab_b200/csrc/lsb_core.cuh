@@ -715,8 +715,8 @@ __device__ __forceinline__ void table_apply_known(const TableView& t, typename T
 // kBarrierPolls times; on timeout it raises kStatusBarrier and returns false
 // so the caller can leave the kernel.
 struct GridBarrier {
-  uint32_t count;  // arrivals in this launch (zeroed before the launch)
-  uint32_t pad;
+  uint32_t count;  // arrivals in this launch (zero when a launch starts)
+  uint32_t exits;  // blocks that have left the launch (see release_counters)
 };
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status,

@@ -962,6 +962,35 @@ __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
   }
 }
 
+// ------------------------------------------------------------ counters
+// A table's counter block (two window-counter sets, the grid barrier and,
+// for region binning, two bin-counter sets) is zero whenever none of the
+// table's kernels runs.  The last block to leave a kernel that used it
+// clears it for the next launch, so no memset launch precedes a batch.
+// Every thread of every block calls this once, as the block's last action.
+__device__ inline void release_counters(WinCounters* cnt, GridBarrier* bar, void* bins,
+                                        uint32_t bin_words) {
+  __syncthreads();
+  int last = 0;
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's counter updates before its exit is counted
+    last = atomicAdd(&bar->exits, 1u) == gridDim.x - 1;
+    if (last) __threadfence();
+  }
+  if (__syncthreads_or(last)) {
+    uint32_t* words = reinterpret_cast<uint32_t*>(cnt);
+    for (uint32_t i = threadIdx.x; i < 2 * sizeof(WinCounters) / 4; i += blockDim.x) words[i] = 0;
+    uint32_t* b = static_cast<uint32_t*>(bins);
+    for (uint32_t i = threadIdx.x; b && i < bin_words; i += blockDim.x) b[i] = 0;
+    if (threadIdx.x == 0) bar->count = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      bar->exits = 0;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- phase E
 // Post-state of mutation p as (present, value).
 template <class Tr>
