@@ -262,6 +262,82 @@ int lsb_set_autotune(lsb_set* s, const uint8_t* types, const uint32_t* keys, boo
 /* container: 0 map, 1 set.  LSB_ERR_STATE when that size was never tuned. */
 int lsb_autotune_lookup(int container, unsigned log2_buckets, lsb_tuning* out);
 
+/* ---- serving: a device-resident request loop over one map ---------------
+ * No counterpart in the reference (lslab only has batched host calls); this
+ * is the KV-store serving form.  lsb_serve_start launches one persistent
+ * kernel that admits waves of queued requests in FIFO order (continuous
+ * batching: requests that arrive while a wave runs join the next one), runs
+ * each wave through the same engine as lsb_map_execute_fused and publishes
+ * completions.  A wave admits the longest queue prefix that fits
+ * max_wave_ops and whose worst-case new slabs (one per put) fit the pool's
+ * free slabs; a request that can never fit (slabs are not returned to the
+ * pool) completes with status LSB_ERR_OOM and no effect.  Ops of a wave run
+ * in request order, so results equal running the requests one after another
+ * in submission order.  Requests, ops and results live in GPU-mapped pinned
+ * host memory; the table and each wave's working copy stay in device memory.
+ * While the loop runs, no other call may use the map.  The loop ends on
+ * lsb_serve_stop (after draining the queue) or after idle_ms without
+ * requests. */
+typedef struct lsb_server lsb_server;
+
+typedef struct lsb_serve_options {
+  uint32_t max_wave_ops;  /* ops per wave; 0 = 2^16; at most the map's max_window */
+  uint32_t ring_requests; /* request slots; 0 = 16384 */
+  uint64_t arena_ops;     /* ops the host-mapped arena holds; 0 = 2^22 */
+  uint32_t idle_ms;       /* loop ends after about this long without requests; 0 = 10000 */
+  uint32_t pad;
+} lsb_serve_options;
+
+typedef struct lsb_serve_stats {
+  uint64_t waves;     /* waves run */
+  uint64_t ops;       /* ops run */
+  uint64_t requests;  /* requests completed (refused ones included) */
+  uint32_t state;     /* 0 never ran, 1 running, 2 drained after stop, 3 idle limit,
+                         4 a grid barrier gave up (see lsb_map_status) */
+  uint32_t pad;
+} lsb_serve_stats;
+
+int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out);
+/* Launches the loop on the server's own stream. */
+int lsb_serve_start(lsb_server* s);
+/* Queues one request of n ops (host pointers; types NULL = all gets, vals
+ * NULL = zeros).  LSB_ERR_STATE when the queue or arena is full: take
+ * results of finished requests, then retry.  *ticket numbers requests from 0. */
+int lsb_serve_submit(lsb_server* s, const uint8_t* types, const uint64_t* keys,
+                     const uint64_t* vals, uint32_t n, uint64_t* ticket);
+/* *done = 1 once the request has finished. */
+int lsb_serve_poll(lsb_server* s, uint64_t ticket, int* done);
+/* Copies a finished request's n results to host memory `out` (may be NULL)
+ * and its status (LSB_OK or LSB_ERR_OOM) to *status, then frees its slot.
+ * Once per ticket; LSB_ERR_STATE when it has not finished. */
+int lsb_serve_take(lsb_server* s, uint64_t ticket, lsb_result* out, int* status);
+/* Drains the queue, ends the loop, waits for it.  Synchronises. */
+int lsb_serve_stop(lsb_server* s, lsb_serve_stats* stats);
+int lsb_serve_destroy(lsb_server* s);
+
+/* Open-loop load generator for the serving benchmark: issues nreq requests
+ * at scheduled times (request i repeats pooled request pool_index[i] and is
+ * due at start + arrival_ns[i]; a full queue delays issue, not the schedule),
+ * takes every result on a second thread and writes each request's latency
+ * (scheduled arrival to observed completion, ns) to latency_ns[i].
+ * results (optional) receives every issued request's results in issue order.
+ * The loop must be running.  Returns the wall time of the run in *wall_ns. */
+typedef struct lsb_serve_load {
+  uint64_t nreq;
+  const uint64_t* arrival_ns;
+  const uint32_t* pool_index;
+  uint32_t pool_size;
+  uint32_t pad;
+  const uint64_t* pool_off; /* first op of each pooled request in the arrays below */
+  const uint32_t* pool_n;   /* ops of each pooled request */
+  const uint8_t* types;
+  const uint64_t* keys;
+  const uint64_t* vals;
+  lsb_result* results;
+} lsb_serve_load;
+int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* load, uint64_t* latency_ns,
+                       uint64_t* wall_ns);
+
 /* ---- misc ------------------------------------------------------------- */
 const char* lsb_error_string(int code);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */

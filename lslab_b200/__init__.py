@@ -26,7 +26,7 @@ from ._lib import (LOCK_FREE, LOCK_RW, LOCK_WRITER, OP_CONTAINS, OP_GET, OP_INSE
                    LsbError)
 
 __all__ = [
-    "Map", "Set", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_CONTAINS", "OP_INSERT",
+    "Map", "Set", "Server", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_CONTAINS", "OP_INSERT",
     "LOCK_WRITER", "LOCK_FREE", "LOCK_RW", "STATUS_OOM", "STATUS_TIMEOUT", "STATUS_CHAIN",
     "STATUS_BARRIER", "STATUS_SCRATCH", "lib",
 ]
@@ -269,3 +269,95 @@ class Set(_Table):
         cnt = C.c_uint64()
         self._call("dump", k.ctypes.data, n, C.byref(cnt), _stream(stream))
         return k[: cnt.value]
+
+
+class Server:
+    """Device-resident request loop over a Map (lsb_serve_*, include/lsb.h).
+
+    Requests are host numpy arrays (types uint8, keys/values uint64); results
+    come back as numpy structured arrays of lsb_result.  While the loop runs,
+    the map must not be used by other calls."""
+
+    RESULT = None
+
+    def __init__(self, m: "Map", max_wave_ops: int = 0, ring_requests: int = 0,
+                 arena_ops: int = 0, idle_ms: int = 0):
+        import numpy as np
+        if Server.RESULT is None:
+            Server.RESULT = np.dtype([("found", "u1"), ("pad", "u1", (7,)), ("value", "<u8")])
+        o = _lib.ServeOptions(int(max_wave_ops), int(ring_requests), int(arena_ops),
+                              int(idle_ms), 0)
+        h = C.c_void_p()
+        _lib.check(lib().lsb_serve_create(m._h, C.byref(o), C.byref(h)), "lsb_serve_create")
+        self._h = h
+        self.map = m
+
+    def start(self):
+        _lib.check(lib().lsb_serve_start(self._h), "lsb_serve_start")
+
+    def submit(self, types, keys, values=None) -> int | None:
+        """Queue one request; returns its ticket, or None when the queue is full."""
+        import numpy as np
+        k = np.ascontiguousarray(keys, np.uint64)
+        t = None if types is None else np.ascontiguousarray(types, np.uint8)
+        v = None if values is None else np.ascontiguousarray(values, np.uint64)
+        ticket = C.c_uint64()
+        rc = lib().lsb_serve_submit(self._h, None if t is None else t.ctypes.data, k.ctypes.data,
+                                    None if v is None else v.ctypes.data, len(k),
+                                    C.byref(ticket))
+        if rc == _lib.LSB_ERR_STATE:
+            return None
+        _lib.check(rc, "lsb_serve_submit")
+        return int(ticket.value)
+
+    def done(self, ticket: int) -> bool:
+        d = C.c_int()
+        _lib.check(lib().lsb_serve_poll(self._h, int(ticket), C.byref(d)), "lsb_serve_poll")
+        return bool(d.value)
+
+    def take(self, ticket: int, n: int):
+        """(results, status) of a finished request of n ops."""
+        import numpy as np
+        out = np.zeros(n, Server.RESULT)
+        st = C.c_int()
+        _lib.check(lib().lsb_serve_take(self._h, int(ticket), out.ctypes.data, C.byref(st)),
+                   "lsb_serve_take")
+        return out, int(st.value)
+
+    def run_load(self, arrival_ns, pool_index, pool_off, pool_n, types, keys, values,
+                 want_results: bool = False):
+        """Open-loop run (lsb_serve_run_load): latencies (ns per request), wall
+        time (ns) and, if asked, all results in issue order."""
+        import numpy as np
+        arr = np.ascontiguousarray(arrival_ns, np.uint64)
+        idx = np.ascontiguousarray(pool_index, np.uint32)
+        poff = np.ascontiguousarray(pool_off, np.uint64)
+        pn = np.ascontiguousarray(pool_n, np.uint32)
+        t = np.ascontiguousarray(types, np.uint8)
+        k = np.ascontiguousarray(keys, np.uint64)
+        v = np.ascontiguousarray(values, np.uint64)
+        res = np.zeros(int(pn[idx].sum()), Server.RESULT) if want_results else None
+        lat = np.zeros(len(arr), np.uint64)
+        ld = _lib.ServeLoad(len(arr), arr.ctypes.data, idx.ctypes.data, len(pn), 0,
+                            poff.ctypes.data, pn.ctypes.data, t.ctypes.data, k.ctypes.data,
+                            v.ctypes.data, None if res is None else res.ctypes.data)
+        wall = C.c_uint64()
+        _lib.check(lib().lsb_serve_run_load(self._h, C.byref(ld), lat.ctypes.data, C.byref(wall)),
+                   "lsb_serve_run_load")
+        return lat, int(wall.value), res
+
+    def stop(self) -> dict:
+        s = _lib.ServeStats()
+        _lib.check(lib().lsb_serve_stop(self._h, C.byref(s)), "lsb_serve_stop")
+        return {"waves": s.waves, "ops": s.ops, "requests": s.requests, "state": s.state}
+
+    def close(self):
+        if self._h is not None:
+            lib().lsb_serve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

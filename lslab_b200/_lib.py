@@ -62,6 +62,42 @@ class Tuning(C.Structure):
     ]
 
 
+class ServeOptions(C.Structure):
+    _fields_ = [
+        ("max_wave_ops", C.c_uint32),
+        ("ring_requests", C.c_uint32),
+        ("arena_ops", C.c_uint64),
+        ("idle_ms", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("waves", C.c_uint64),
+        ("ops", C.c_uint64),
+        ("requests", C.c_uint64),
+        ("state", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+class ServeLoad(C.Structure):
+    _fields_ = [
+        ("nreq", C.c_uint64),
+        ("arrival_ns", C.c_void_p),
+        ("pool_index", C.c_void_p),
+        ("pool_size", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("pool_off", C.c_void_p),
+        ("pool_n", C.c_void_p),
+        ("types", C.c_void_p),
+        ("keys", C.c_void_p),
+        ("vals", C.c_void_p),
+        ("results", C.c_void_p),
+    ]
+
+
 _lib: C.CDLL | None = None
 
 _P = C.c_void_p
@@ -114,6 +150,14 @@ _SIGS = {
     "lsb_set_capture_fused": (C.c_int, [_P, _P, _P, _P, _SZ, C.POINTER(_P)]),
     "lsb_graph_launch": (C.c_int, [_P, _P]),
     "lsb_graph_destroy": (C.c_int, [_P]),
+    "lsb_serve_create": (C.c_int, [_P, C.POINTER(ServeOptions), C.POINTER(_P)]),
+    "lsb_serve_start": (C.c_int, [_P]),
+    "lsb_serve_submit": (C.c_int, [_P, _P, _P, _P, _U32, C.POINTER(_U64)]),
+    "lsb_serve_poll": (C.c_int, [_P, _U64, C.POINTER(C.c_int)]),
+    "lsb_serve_take": (C.c_int, [_P, _U64, _P, C.POINTER(C.c_int)]),
+    "lsb_serve_stop": (C.c_int, [_P, C.POINTER(ServeStats)]),
+    "lsb_serve_destroy": (C.c_int, [_P]),
+    "lsb_serve_run_load": (C.c_int, [_P, C.POINTER(ServeLoad), _P, C.POINTER(_U64)]),
     "lsb_error_string": (C.c_char_p, [C.c_int]),
     "lsb_version": (C.c_int, []),
 }

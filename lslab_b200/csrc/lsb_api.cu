@@ -3,6 +3,7 @@
 // stream; argument errors are returned, device errors land in the table's
 // status word.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -105,14 +106,16 @@ __device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t 
   tr[at++] = (ns << 8) | ((uint64_t)(wi & 0x3F) << 2) | ph;
 }
 
+// All windows of one batch.  `seq` counts the grid barriers this launch has
+// passed (shared with a caller that runs several batches in one launch).
 template <class Tr, int P>
 __device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
-                              GridBarrier* bar, uint32_t* smem) {
+                              GridBarrier* bar, uint32_t* smem, uint32_t& seq) {
   const uint32_t nblocks = gridDim.x;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   const uint32_t warp = tid >> 5, nwarps = nt >> 5;
   const uint32_t nwin = (job.base.n + job.window - 1) / job.window;
-  uint32_t tat = 0, seq = 0;
+  uint32_t tat = 0;
   // Window epochs live on the device so that a replayed CUDA graph of this
   // launch never reuses one: the fused path takes odd epochs 2f+1 (f = fused
   // windows so far), the per-phase path even ones from the host.  When the
@@ -198,8 +201,183 @@ template <class Tr, int P>
 __global__ void __launch_bounds__(1024, 1)
     k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
-  fused_windows<Tr, P>(t, sc, job, bar, smem);
+  uint32_t seq = 0;
+  fused_windows<Tr, P>(t, sc, job, bar, smem, seq);
   release_counters(sc.cnt, bar, job.bins, 2 * sizeof(BinCounters) / 4);
+}
+
+// ------------------------------------------------------------------ serving
+// A device-resident request loop over one map (lsb_serve_*): one persistent
+// cooperative launch admits waves of queued requests (continuous batching:
+// whatever arrived while the previous wave ran joins the next one), runs each
+// wave through the batch engine as one window and publishes completions.
+// Requests, their ops and their results sit in GPU-mapped pinned host memory,
+// where a KV server's network layer would deliver them; the table, the pool
+// and each wave's working copy stay in HBM.  Ops of a wave run in request
+// order (FIFO admission), so a wave equals running its requests one after
+// another.
+struct ServeCtl {     // host-mapped
+  uint64_t submitted;  // requests published by the host (monotonic)
+  uint64_t completed;  // requests finished by the device (monotonic)
+  uint64_t waves;      // waves run
+  uint64_t ops;        // ops run
+  uint32_t stop;       // host: end the loop once the queue is drained
+  uint32_t state;      // device: see lsb_serve_stats.state
+};
+
+struct ServeReq {     // one request slot, host-mapped
+  uint64_t op_off;     // first op in the arena (monotonic op count; slot = off % arena)
+  uint32_t n;          // ops
+  uint32_t puts;       // puts among them: the request's worst-case new slabs
+  int32_t status;      // device: LSB_OK, or LSB_ERR_OOM when the pool cannot take it
+  uint32_t pad;
+};
+
+struct WaveDesc {     // device: the wave that thread 0 admitted
+  uint64_t first;      // first request of the wave
+  uint64_t op_off;     // its first op in the arena
+  uint32_t nreq;       // requests completed by this wave
+  uint32_t nops;       // ops run (0 when the head request was refused)
+  uint32_t stop;       // 1 drained after a stop request, 2 idle limit
+  uint32_t pad;
+};
+
+struct ServeJob {
+  ServeCtl* ctl;
+  ServeReq* ring;
+  uint64_t ring_cap;
+  const uint8_t* a_types;   // host-mapped op arena
+  const uint64_t* a_keys;
+  const uint64_t* a_vals;
+  lsb_result* a_out;
+  uint64_t arena_cap;
+  uint8_t* d_types;         // HBM working copy of a wave
+  uint64_t* d_keys;
+  uint64_t* d_vals;
+  lsb_result* d_out;
+  WaveDesc* wave;
+  uint32_t max_wave_ops;
+  uint32_t idle_polls;
+  FusedJob<MapTraits> fj;   // engine parameters; base is set per wave
+};
+
+__device__ __forceinline__ uint64_t ld_acquire_sys_u64(const uint64_t* p) {
+  uint64_t r;
+  asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(r) : "l"(p) : "memory");
+  return r;
+}
+
+__device__ __forceinline__ void st_release_sys_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Thread 0 of block 0: wait (bounded) for requests, then admit the longest
+// FIFO prefix that fits the wave's op limit and whose worst-case new slabs
+// (one per put) fit the pool's free slabs.  A head request that can never fit
+// the pool (slabs are not returned) is refused alone with LSB_ERR_OOM.
+__device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head) {
+  WaveDesc wd{};
+  wd.first = head;
+  uint64_t sub = 0;
+  for (uint32_t it = 0;; ++it) {
+    sub = ld_acquire_sys_u64(&j.ctl->submitted);
+    if (sub > head) break;
+    if (*(volatile uint32_t*)&j.ctl->stop) {
+      wd.stop = 1;
+      *j.wave = wd;
+      return;
+    }
+    if (it >= j.idle_polls) {
+      wd.stop = 2;
+      *j.wave = wd;
+      return;
+    }
+    __nanosleep(it < 64 ? 128 : 2048);
+  }
+  const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
+  uint64_t budget = limit > cursor ? limit - cursor : 0;
+  uint32_t nops = 0, nreq = 0;
+  for (uint64_t r = head; r < sub && r - head < j.ring_cap; ++r) {
+    volatile ServeReq* q = &j.ring[r % j.ring_cap];
+    const uint32_t n = q->n, puts = q->puts;
+    if (nreq == 0) wd.op_off = q->op_off;
+    if (puts > budget) {
+      if (nreq == 0) {
+        q->status = LSB_ERR_OOM;
+        nreq = 1;
+      }
+      break;
+    }
+    if (nops + n > j.max_wave_ops) break;  // n <= max_wave_ops: submit checks it
+    q->status = LSB_OK;
+    budget -= puts;
+    nops += n;
+    ++nreq;
+  }
+  wd.nreq = nreq;
+  wd.nops = nops;
+  *j.wave = wd;
+}
+
+template <int P>
+__global__ void __launch_bounds__(1024, 1)
+    k_serve(TableView t, Scratch sc, ServeJob j, GridBarrier* bar) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  uint32_t seq = 0;
+  uint64_t head = 0;  // meaningful in thread 0
+  if (tid == 0) {
+    head = ld_acquire_sys_u64(&j.ctl->completed);
+    *(volatile uint32_t*)&j.ctl->state = 1;
+  }
+  for (;;) {
+    if (tid == 0) serve_admit(t, j, head);
+    if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+    const uint64_t first = ld_cg_u64(&j.wave->first), op_off = ld_cg_u64(&j.wave->op_off);
+    const uint32_t nreq = ld_cg_u32(&j.wave->nreq), nops = ld_cg_u32(&j.wave->nops);
+    const uint32_t stop = ld_cg_u32(&j.wave->stop);
+    if (stop) {
+      if (tid == 0) *(volatile uint32_t*)&j.ctl->state = stop == 1 ? 2 : 3;
+      break;
+    }
+    if (nops) {
+      // the wave's ops into HBM (the arena is re-read each time: .cv loads)
+      for (uint32_t i = tid; i < nops; i += nt) {
+        const uint64_t pos = (op_off + i) % j.arena_cap;
+        j.d_types[i] = __ldcv(j.a_types + pos);
+        j.d_keys[i] = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos);
+        j.d_vals[i] = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos);
+      }
+      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+      FusedJob<MapTraits> fj = j.fj;
+      fj.base.types = j.d_types;
+      fj.base.keys = j.d_keys;
+      fj.base.vals = j.d_vals;
+      fj.base.out = j.d_out;
+      fj.base.n = nops;
+      fused_windows<MapTraits, P>(t, sc, fj, bar, smem, seq);
+      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+      for (uint32_t i = tid; i < nops; i += nt) {
+        const uint64_t pos = (op_off + i) % j.arena_cap;
+        const ulonglong2 r = ld_cg_v2u64(&j.d_out[i]);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(j.a_out + pos);
+        __stcs(dst, r.x);
+        __stcs(dst + 1, r.y);
+      }
+      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+    }
+    if (tid == 0) {
+      win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
+      __threadfence_system();          // results before the completion count
+      *(volatile uint64_t*)&j.ctl->waves = *(volatile uint64_t*)&j.ctl->waves + 1;
+      *(volatile uint64_t*)&j.ctl->ops = *(volatile uint64_t*)&j.ctl->ops + nops;
+      head = first + nreq;
+      st_release_sys_u64(&j.ctl->completed, head);
+    }
+  }
+  if (tid == 0 && (*(volatile uint32_t*)t.status & kStatusBarrier))
+    *(volatile uint32_t*)&j.ctl->state = 4;
+  release_counters(sc.cnt, bar, j.fj.bins, 2 * sizeof(BinCounters) / 4);
 }
 
 // Live-entry count and dump: one thread per bucket walks the chain.
@@ -801,6 +979,56 @@ void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buc
   *buckets = m->t.buckets;
 }
 
+// ------------------------------------------------------------------ serving
+// Host side of the request loop (see k_serve).  One producer may submit while
+// another thread takes results; both advance FIFO cursors.
+struct lsb_server {
+  lsb_map* map = nullptr;
+  int device = 0;
+  ServeCtl* ctl = nullptr;    // host pointers (pinned, mapped)
+  ServeReq* ring = nullptr;
+  uint8_t* a_types = nullptr;
+  uint64_t* a_keys = nullptr;
+  uint64_t* a_vals = nullptr;
+  lsb_result* a_out = nullptr;
+  uint64_t ring_cap = 0, arena_cap = 0;
+  uint32_t max_wave_ops = 0, idle_polls = 0;
+  uint8_t* d_types = nullptr;  // HBM working copy of a wave
+  uint64_t* d_keys = nullptr;
+  uint64_t* d_vals = nullptr;
+  lsb_result* d_out = nullptr;
+  WaveDesc* d_wave = nullptr;
+  cudaStream_t stream = nullptr;
+  bool running = false;
+  std::mutex submit_mu;
+  uint64_t next_req = 0, next_op = 0;         // producer cursors
+  std::atomic<uint64_t> freed_req{0}, freed_op{0};  // taken (reclaimable) prefix
+  std::vector<uint8_t> taken;                  // per ring slot: results taken
+  std::mutex take_mu;
+
+  void release() {
+    cudaFreeHost(ctl);
+    cudaFreeHost(ring);
+    cudaFreeHost(a_types);
+    cudaFreeHost(a_keys);
+    cudaFreeHost(a_vals);
+    cudaFreeHost(a_out);
+    cudaFree(d_types);
+    cudaFree(d_keys);
+    cudaFree(d_vals);
+    cudaFree(d_out);
+    cudaFree(d_wave);
+  }
+};
+
+namespace {
+template <class T>
+T* dev_ptr(T* host) {
+  void* d = nullptr;
+  return cudaHostGetDevicePointer(&d, host, 0) == cudaSuccess ? static_cast<T*>(d) : nullptr;
+}
+}  // namespace
+
 extern "C" {
 
 // ------------------------------------------------------------------ map
@@ -1095,5 +1323,231 @@ const char* lsb_error_string(int code) {
 }
 
 int lsb_version(void) { return 100; }
+
+/* ---------------------------------------------------------------- serving */
+int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out) {
+  if (!m || !out) return LSB_ERR_ARG;
+  *out = nullptr;
+  lsb_serve_options o{};
+  if (opt) o = *opt;
+  const uint32_t wave = o.max_wave_ops ? o.max_wave_ops : (1u << 16);
+  const uint64_t ring = o.ring_requests ? o.ring_requests : 16384;
+  const uint64_t arena = o.arena_ops ? o.arena_ops : (1ull << 22);
+  if (wave > m->t.sc.max_window || wave < 1 || arena < wave || ring > (1ull << 24) ||
+      arena > (1ull << 32))
+    return LSB_ERR_ARG;
+  lsb_server* s = new (std::nothrow) lsb_server;
+  if (!s) return LSB_ERR_OOM;
+  s->map = m;
+  s->device = m->t.device;
+  s->ring_cap = ring;
+  s->arena_cap = arena;
+  s->max_wave_ops = wave;
+  // idle limit in polls of ~2 us (the admit loop's back-off)
+  s->idle_polls = (uint32_t)std::min<uint64_t>(0xFFFFFFFFull,
+                                                (uint64_t)(o.idle_ms ? o.idle_ms : 10000) * 500);
+  s->taken.assign(ring, 0);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  const unsigned fl = cudaHostAllocMapped;
+  bool ok =
+      cudaHostAlloc((void**)&s->ctl, sizeof(ServeCtl), fl) == cudaSuccess &&
+      cudaHostAlloc((void**)&s->ring, sizeof(ServeReq) * ring, fl) == cudaSuccess &&
+      cudaHostAlloc((void**)&s->a_types, arena, fl) == cudaSuccess &&
+      cudaHostAlloc((void**)&s->a_keys, 8 * arena, fl) == cudaSuccess &&
+      cudaHostAlloc((void**)&s->a_vals, 8 * arena, fl) == cudaSuccess &&
+      cudaHostAlloc((void**)&s->a_out, sizeof(lsb_result) * arena, fl) == cudaSuccess &&
+      cudaMalloc(&s->d_types, wave) == cudaSuccess &&
+      cudaMalloc(&s->d_keys, 8ull * wave) == cudaSuccess &&
+      cudaMalloc(&s->d_vals, 8ull * wave) == cudaSuccess &&
+      cudaMalloc(&s->d_out, sizeof(lsb_result) * (size_t)wave) == cudaSuccess &&
+      cudaMalloc(&s->d_wave, sizeof(WaveDesc)) == cudaSuccess &&
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+  cudaSetDevice(prev);
+  if (!ok) {
+    cudaGetLastError();
+    s->release();
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return LSB_ERR_OOM;
+  }
+  std::memset(s->ctl, 0, sizeof(ServeCtl));
+  std::memset(s->ring, 0, sizeof(ServeReq) * ring);
+  *out = s;
+  return LSB_OK;
+}
+
+int lsb_serve_start(lsb_server* s) {
+  if (!s) return LSB_ERR_ARG;
+  if (s->running) return LSB_ERR_STATE;
+  auto& tb = s->map->t;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  LSB_CK(cudaSetDevice(s->device));
+  s->ctl->stop = 0;
+  s->ctl->state = 0;
+  ServeJob j{};
+  j.ctl = dev_ptr(s->ctl);
+  j.ring = dev_ptr(s->ring);
+  j.ring_cap = s->ring_cap;
+  j.a_types = dev_ptr(s->a_types);
+  j.a_keys = dev_ptr(s->a_keys);
+  j.a_vals = dev_ptr(s->a_vals);
+  j.a_out = dev_ptr(s->a_out);
+  j.arena_cap = s->arena_cap;
+  j.d_types = s->d_types;
+  j.d_keys = s->d_keys;
+  j.d_vals = s->d_vals;
+  j.d_out = s->d_out;
+  j.wave = s->d_wave;
+  j.max_wave_ops = s->max_wave_ops;
+  j.idle_polls = s->idle_polls;
+  if (!j.ctl || !j.ring || !j.a_types || !j.a_keys || !j.a_vals || !j.a_out) {
+    cudaSetDevice(prev);
+    return LSB_ERR_CUDA;
+  }
+  FusedJob<MapTraits>& fj = j.fj;
+  fj.base = tb.window(s->d_types, 0, s->d_keys, 1, s->d_vals, 1, s->d_out, kOutResult,
+                      s->max_wave_ops);
+  fj.window = tb.sc.max_window;
+  fj.fused_epoch = tb.fused_epoch;
+  fj.chunk = tb.tune.chunk;
+  fj.dedup = tb.tune.dedup;
+  fj.split_q16 = tb.split_q16;
+  fj.trace = nullptr;
+  fj.bins = tb.bins;
+  fj.binned = 0;
+  fj.bin_shift = 0;
+  const int per_sm_grid = tb.fused_grid();  // same occupancy as the fused kernel
+  if (per_sm_grid <= 0) {
+    cudaSetDevice(prev);
+    return LSB_ERR_STATE;
+  }
+  int per_sm = 0;
+  const void* f = tb.tune.prefetch == 0 ? (const void*)k_serve<1>
+                : tb.tune.prefetch == 1 ? (const void*)k_serve<2> : (const void*)k_serve<3>;
+  if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortSmemBytes) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, (int)tb.tune.block,
+                                                    kSortSmemBytes) != cudaSuccess ||
+      per_sm <= 0) {
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    return LSB_ERR_CUDA;
+  }
+  TableView tv = tb.view();
+  Scratch scv = tb.sc;
+  GridBarrier* b = tb.bar;
+  void* args[] = {&tv, &scv, &j, &b};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(per_sm * tb.num_sms);
+  cfg.blockDim = dim3(tb.tune.block);
+  cfg.dynamicSmemBytes = kSortSmemBytes;
+  cfg.stream = s->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelExC(&cfg, f, args);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return LSB_ERR_CUDA;
+  }
+  s->running = true;
+  return LSB_OK;
+}
+
+int lsb_serve_submit(lsb_server* s, const uint8_t* types, const uint64_t* keys,
+                     const uint64_t* vals, uint32_t n, uint64_t* ticket) {
+  if (!s || !keys || !ticket || n == 0 || n > s->max_wave_ops) return LSB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->submit_mu);
+  const uint64_t freed_req = s->freed_req.load(std::memory_order_acquire);
+  const uint64_t freed_op = s->freed_op.load(std::memory_order_acquire);
+  if (s->next_req - freed_req >= s->ring_cap || s->next_op + n - freed_op > s->arena_cap)
+    return LSB_ERR_STATE;  // full: take results, then retry
+  uint32_t puts = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint64_t pos = (s->next_op + i) % s->arena_cap;
+    const uint8_t ty = types ? types[i] : (uint8_t)kOpRead;
+    s->a_types[pos] = ty;
+    s->a_keys[pos] = keys[i];
+    s->a_vals[pos] = vals ? vals[i] : 0;
+    puts += ty == kOpWrite;
+  }
+  ServeReq& q = s->ring[s->next_req % s->ring_cap];
+  q.op_off = s->next_op;
+  q.n = n;
+  q.puts = puts;
+  q.status = -1;
+  *ticket = s->next_req;
+  s->next_op += n;
+  ++s->next_req;
+  std::atomic_thread_fence(std::memory_order_release);
+  __atomic_store_n(&s->ctl->submitted, s->next_req, __ATOMIC_RELEASE);
+  return LSB_OK;
+}
+
+int lsb_serve_poll(lsb_server* s, uint64_t ticket, int* done) {
+  if (!s || !done) return LSB_ERR_ARG;
+  *done = __atomic_load_n(&s->ctl->completed, __ATOMIC_ACQUIRE) > ticket;
+  return LSB_OK;
+}
+
+int lsb_serve_take(lsb_server* s, uint64_t ticket, lsb_result* out, int* status) {
+  if (!s) return LSB_ERR_ARG;
+  if (__atomic_load_n(&s->ctl->completed, __ATOMIC_ACQUIRE) <= ticket) return LSB_ERR_STATE;
+  std::lock_guard<std::mutex> lk(s->take_mu);
+  const uint64_t fr = s->freed_req.load(std::memory_order_relaxed);
+  if (ticket < fr || ticket - fr >= s->ring_cap) return LSB_ERR_ARG;
+  const ServeReq& q = s->ring[ticket % s->ring_cap];
+  if (s->taken[ticket % s->ring_cap]) return LSB_ERR_STATE;
+  if (status) *status = q.status;
+  if (out) {
+    for (uint32_t i = 0; i < q.n; ++i) out[i] = s->a_out[(q.op_off + i) % s->arena_cap];
+  }
+  s->taken[ticket % s->ring_cap] = 1;
+  // reclaim the FIFO prefix of taken requests
+  uint64_t r = fr, op = s->freed_op.load(std::memory_order_relaxed);
+  const uint64_t done = __atomic_load_n(&s->ctl->completed, __ATOMIC_ACQUIRE);
+  while (r < done && s->taken[r % s->ring_cap]) {
+    const ServeReq& d = s->ring[r % s->ring_cap];
+    s->taken[r % s->ring_cap] = 0;
+    op = d.op_off + d.n;
+    ++r;
+  }
+  s->freed_op.store(op, std::memory_order_release);
+  s->freed_req.store(r, std::memory_order_release);
+  return LSB_OK;
+}
+
+int lsb_serve_stop(lsb_server* s, lsb_serve_stats* stats) {
+  if (!s) return LSB_ERR_ARG;
+  int rc = LSB_OK;
+  if (s->running) {
+    __atomic_store_n(&s->ctl->stop, 1u, __ATOMIC_RELEASE);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) rc = LSB_ERR_CUDA;
+    s->running = false;
+  }
+  if (stats) {
+    stats->waves = s->ctl->waves;
+    stats->ops = s->ctl->ops;
+    stats->requests = s->ctl->completed;
+    stats->state = s->ctl->state;
+    stats->pad = 0;
+  }
+  return rc;
+}
+
+int lsb_serve_destroy(lsb_server* s) {
+  if (!s) return LSB_ERR_ARG;
+  if (s->running) lsb_serve_stop(s, nullptr);
+  s->release();
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return LSB_OK;
+}
 
 }  // extern "C"
