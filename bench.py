@@ -50,9 +50,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="zipf9505", choices=["zipf9505", "batches"],
+    ap.add_argument("--workload", default="zipf9505", choices=["zipf9505", "batches", "serving"],
                     help="zipf9505: the headline line; batches: 4096 uneven mixed batches in "
-                         "one graph-captured fused launch vs per-op-type calls")
+                         "one graph-captured fused launch vs per-op-type calls; serving: the "
+                         "request loop under open-loop Poisson load")
+    ap.add_argument("--wave-ops", type=int, default=1 << 16, help="serving: ops per wave")
+    ap.add_argument("--serve-seconds", type=float, default=0.4,
+                    help="serving: offered-load duration of each sweep point")
+    ap.add_argument("--serve-loads", default="0.1,0.3,0.5,0.7,0.9,1.0",
+                    help="serving: offered loads as fractions of the measured peak")
     ap.add_argument("--nbatches", type=int, default=4096)
     ap.add_argument("--buckets-log2", type=int, default=22)
     ap.add_argument("--prefill-log2", type=int, default=26)
@@ -676,6 +682,65 @@ def run_batches(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_serving(args, world, rank, local):
+    """Serving (map 2^25 buckets, slab pool capped at 24 GB): requests of
+    uniform [1, 4096] ops, 50/50 get/put, Zipf 0.99 over 2^28 keys, fed by the
+    open-loop generator (lsb_serve_run_load) from a pool of 4096 requests.
+    Peak = throughput with the queue never empty; then Poisson arrivals at
+    fractions of that peak, each point reporting achieved Mops/s and the
+    p50/p99/p999 latency from scheduled arrival to observed completion."""
+    import lslab_b200 as L
+    from lslab_b200 import workload as W
+    from lslab_b200.shard import rank_seed
+
+    seed = rank_seed(args.seed, rank)
+    pool_slabs = 24_000_000_000 // 480
+    m = L.Map(25, pool_slabs)
+    srv = L.Server(m, max_wave_ops=args.wave_ops, ring_requests=16384, arena_ops=1 << 22)
+    off, n, t, k, v = W.serving_pool(seed, 4096)
+    mean_n = float(n.mean())
+    rng = np.random.default_rng(seed)
+    srv.start()
+
+    def run(nreq, arrival):
+        idx = rng.integers(0, len(n), size=nreq).astype(np.uint32)
+        lat, wall, _ = srv.run_load(arrival, idx, off, n, t, k, v)
+        ops = int(n[idx].astype(np.uint64).sum())
+        return lat, wall, ops
+
+    run(512, np.zeros(512, np.uint64))  # warm-up
+    peak_req = 8192
+    _, wall, ops = run(peak_req, np.zeros(peak_req, np.uint64))
+    peak = ops / (wall * 1e-9)
+    sweep = []
+    for f in [float(x) for x in args.serve_loads.split(",")]:
+        lam = f * peak / mean_n  # requests per second
+        nreq = max(256, int(lam * args.serve_seconds))
+        arrival = np.cumsum(rng.exponential(1e9 / lam, size=nreq)).astype(np.uint64)
+        lat, wall, ops = run(nreq, arrival)
+        us = lat / 1e3
+        sweep.append({"load": f, "offered_mops": round(f * peak / 1e6, 1),
+                      "achieved_mops": round(ops / (wall * 1e-9) / 1e6, 1), "requests": nreq,
+                      "p50_us": round(float(np.percentile(us, 50)), 1),
+                      "p99_us": round(float(np.percentile(us, 99)), 1),
+                      "p999_us": round(float(np.percentile(us, 99.9)), 1)})
+    stats = srv.stop()
+    srv.close()
+    at70 = [p for p in sweep if abs(p["load"] - 0.7) < 1e-9]
+    line = {
+        "workload": "serving",
+        "description": ("map 2^25 buckets, slab pool capped at 24 GB; requests uniform [1, 4096] "
+                        "ops, 50/50 get/put, Zipf 0.99 over 2^28 keys; open-loop Poisson "
+                        "arrivals; latency = scheduled arrival to observed completion"),
+        "wave_ops": args.wave_ops, "peak_mops": round(peak / 1e6, 1),
+        "p99_us_at_70pct": at70[0]["p99_us"] if at70 else None,
+        "sweep": sweep, "loop": stats, "device_status": m.status(),
+        "pool_slabs_used": m.pool_usage()[0] if hasattr(m, "pool_usage") else None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -683,6 +748,8 @@ def main():
         run_reference(args, world, rank, local)
     elif args.workload == "batches":
         run_batches(args, world, rank, local)
+    elif args.workload == "serving":
+        run_serving(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
     if world > 1:

@@ -186,8 +186,13 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     }
     trace_mark(job.trace, tat, wi, 2);
     if (has_mut) {
-      phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
-      phase_resolve_reads<Tr>(sc, w, tid, nt);
+      // mutations and later reads resolve independently: half the grid each,
+      // so a small window pays one latency chain instead of two
+      const uint32_t half = (nt / 64) * 32;
+      if (tid < half)
+        phase_resolve_mutations<Tr>(t, sc, w, tid, half);
+      else
+        phase_resolve_reads<Tr>(sc, w, tid - half, nt - half);
     }
     // Before the next window: its probes must see this window's writes, and
     // its first thread resets this window's counter set, which every block
@@ -251,10 +256,9 @@ struct ServeJob {
   const uint64_t* a_vals;
   lsb_result* a_out;
   uint64_t arena_cap;
-  uint8_t* d_types;         // HBM working copy of a wave
+  uint8_t* d_types;         // HBM working copy of a wave's ops
   uint64_t* d_keys;
   uint64_t* d_vals;
-  lsb_result* d_out;
   WaveDesc* wave;
   uint32_t max_wave_ops;
   uint32_t idle_polls;
@@ -271,52 +275,102 @@ __device__ __forceinline__ void st_release_sys_u64(uint64_t* p, uint64_t v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Thread 0 of block 0: wait (bounded) for requests, then admit the longest
-// FIFO prefix that fits the wave's op limit and whose worst-case new slabs
-// (one per put) fit the pool's free slabs.  A head request that can never fit
-// the pool (slabs are not returned) is refused alone with LSB_ERR_OOM.
+// Warp 0 of block 0: wait (bounded) for requests, then admit the longest
+// FIFO prefix that fits the wave's op limit, whose ops are contiguous in the
+// arena (the host never splits a request across the arena's end) and whose
+// worst-case new slabs (one per put) fit the pool's free slabs.  Lanes read
+// 32 descriptors at a time and admit by warp prefix sums.  A head request
+// that can never fit the pool (slabs are not returned) is refused alone with
+// LSB_ERR_OOM.
 __device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head) {
+  const uint32_t lane = threadIdx.x & 31;
   WaveDesc wd{};
   wd.first = head;
   uint64_t sub = 0;
-  for (uint32_t it = 0;; ++it) {
-    sub = ld_acquire_sys_u64(&j.ctl->submitted);
-    if (sub > head) break;
-    if (*(volatile uint32_t*)&j.ctl->stop) {
-      wd.stop = 1;
-      *j.wave = wd;
-      return;
+  uint32_t stop = 0;
+  if (lane == 0) {
+    for (uint32_t it = 0;; ++it) {
+      sub = ld_acquire_sys_u64(&j.ctl->submitted);
+      if (sub > head) break;
+      if (*(volatile uint32_t*)&j.ctl->stop) {
+        stop = 1;
+        break;
+      }
+      if (it >= j.idle_polls) {
+        stop = 2;
+        break;
+      }
+      __nanosleep(it < 64 ? 128 : 2048);
     }
-    if (it >= j.idle_polls) {
-      wd.stop = 2;
-      *j.wave = wd;
-      return;
-    }
-    __nanosleep(it < 64 ? 128 : 2048);
   }
-  const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
-  uint64_t budget = limit > cursor ? limit - cursor : 0;
+  sub = __shfl_sync(0xFFFFFFFFu, sub, 0);
+  stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
+  if (stop) {
+    if (lane == 0) {
+      wd.stop = stop;
+      *j.wave = wd;
+    }
+    return;
+  }
+  uint64_t budget = 0;
+  if (lane == 0) {
+    const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
+    budget = limit > cursor ? limit - cursor : 0;
+  }
+  budget = __shfl_sync(0xFFFFFFFFu, budget, 0);
+  const uint64_t end = min(sub, head + j.ring_cap);
   uint32_t nops = 0, nreq = 0;
-  for (uint64_t r = head; r < sub && r - head < j.ring_cap; ++r) {
+  uint64_t next_off = 0;
+  for (uint64_t base = head; base < end; base += 32) {
+    const uint64_t r = base + lane;
+    const bool valid = r < end;
     volatile ServeReq* q = &j.ring[r % j.ring_cap];
-    const uint32_t n = q->n, puts = q->puts;
-    if (nreq == 0) wd.op_off = q->op_off;
-    if (puts > budget) {
+    const uint64_t off = valid ? q->op_off : 0;
+    const uint32_t n = valid ? q->n : 0, puts = valid ? q->puts : 0;
+    if (base == head) next_off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    // inclusive prefix sums of ops and puts over the lanes
+    uint64_t cn = n, cp = puts;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint64_t yn = __shfl_up_sync(0xFFFFFFFFu, cn, d);
+      const uint64_t yp = __shfl_up_sync(0xFFFFFFFFu, cp, d);
+      if (lane >= (uint32_t)d) {
+        cn += yn;
+        cp += yp;
+      }
+    }
+    // contiguous: this request starts where the previous one ends
+    const uint64_t prev_end = __shfl_up_sync(0xFFFFFFFFu, off + n, 1);
+    const bool contiguous = lane == 0 ? off == next_off : off == prev_end;
+    const bool fits = valid && contiguous && nops + cn <= j.max_wave_ops && cp <= budget;
+    const uint32_t bad = __ballot_sync(0xFFFFFFFFu, !fits);
+    const uint32_t take = bad ? (uint32_t)__ffs(bad) - 1 : 32u;
+    if (lane < take) q->status = LSB_OK;
+    if (take == 0) {
+      if (nreq == 0 && valid && lane == 0 && puts > budget) {
+        q->status = LSB_ERR_OOM;  // refused alone: no op of it runs
+        wd.op_off = off;
+        wd.nreq = 1;
+        wd.nops = 0;
+        *j.wave = wd;
+      }
       if (nreq == 0) {
-        q->status = LSB_ERR_OOM;
-        nreq = 1;
+        if (__shfl_sync(0xFFFFFFFFu, valid && puts > budget, 0)) return;
       }
       break;
     }
-    if (nops + n > j.max_wave_ops) break;  // n <= max_wave_ops: submit checks it
-    q->status = LSB_OK;
-    budget -= puts;
-    nops += n;
-    ++nreq;
+    if (nreq == 0) wd.op_off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    nops += (uint32_t)__shfl_sync(0xFFFFFFFFu, cn, take - 1);
+    budget -= __shfl_sync(0xFFFFFFFFu, cp, take - 1);
+    next_off = __shfl_sync(0xFFFFFFFFu, off + n, take - 1);
+    nreq += take;
+    if (take < 32) break;
   }
-  wd.nreq = nreq;
-  wd.nops = nops;
-  *j.wave = wd;
+  if (lane == 0) {
+    wd.nreq = nreq;
+    wd.nops = nops;
+    *j.wave = wd;
+  }
 }
 
 template <int P>
@@ -325,13 +379,16 @@ __global__ void __launch_bounds__(1024, 1)
   extern __shared__ uint32_t smem[];
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
   uint32_t seq = 0;
-  uint64_t head = 0;  // meaningful in thread 0
+  uint64_t head = 0;  // meaningful in warp 0 of block 0
+  uint64_t waves = 0, ops = 0;  // meaningful in thread 0
+  if (tid < 32) head = ld_acquire_sys_u64(&j.ctl->completed);
   if (tid == 0) {
-    head = ld_acquire_sys_u64(&j.ctl->completed);
-    *(volatile uint32_t*)&j.ctl->state = 1;
+    waves = *(volatile uint64_t*)&j.ctl->waves;
+    ops = *(volatile uint64_t*)&j.ctl->ops;
   }
+  if (tid == 0) *(volatile uint32_t*)&j.ctl->state = 1;
   for (;;) {
-    if (tid == 0) serve_admit(t, j, head);
+    if (tid < 32) serve_admit(t, j, head);
     if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     const uint64_t first = ld_cg_u64(&j.wave->first), op_off = ld_cg_u64(&j.wave->op_off);
     const uint32_t nreq = ld_cg_u32(&j.wave->nreq), nops = ld_cg_u32(&j.wave->nops);
@@ -341,37 +398,36 @@ __global__ void __launch_bounds__(1024, 1)
       break;
     }
     if (nops) {
-      // the wave's ops into HBM (the arena is re-read each time: .cv loads)
+      // the wave's ops (contiguous in the arena) into HBM; .cv loads because
+      // the host rewrites arena slots between waves
+      const uint64_t pos = op_off % j.arena_cap;
       for (uint32_t i = tid; i < nops; i += nt) {
-        const uint64_t pos = (op_off + i) % j.arena_cap;
-        j.d_types[i] = __ldcv(j.a_types + pos);
-        j.d_keys[i] = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos);
-        j.d_vals[i] = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos);
+        // all three loads before any store: they cross PCIe together
+        const uint8_t ty = __ldcv(j.a_types + pos + i);
+        const uint64_t key = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos + i);
+        const uint64_t val = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos + i);
+        j.d_types[i] = ty;
+        j.d_keys[i] = key;
+        j.d_vals[i] = val;
       }
       if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
       FusedJob<MapTraits> fj = j.fj;
       fj.base.types = j.d_types;
       fj.base.keys = j.d_keys;
       fj.base.vals = j.d_vals;
-      fj.base.out = j.d_out;
+      fj.base.out = j.a_out + pos;  // results go straight to the host-mapped arena
       fj.base.n = nops;
       fused_windows<MapTraits, P>(t, sc, fj, bar, smem, seq);
       if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
-      for (uint32_t i = tid; i < nops; i += nt) {
-        const uint64_t pos = (op_off + i) % j.arena_cap;
-        const ulonglong2 r = ld_cg_v2u64(&j.d_out[i]);
-        unsigned long long* dst = reinterpret_cast<unsigned long long*>(j.a_out + pos);
-        __stcs(dst, r.x);
-        __stcs(dst + 1, r.y);
-      }
-      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     }
+    if (tid < 32) head = first + nreq;
     if (tid == 0) {
       win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
       __threadfence_system();          // results before the completion count
-      *(volatile uint64_t*)&j.ctl->waves = *(volatile uint64_t*)&j.ctl->waves + 1;
-      *(volatile uint64_t*)&j.ctl->ops = *(volatile uint64_t*)&j.ctl->ops + nops;
-      head = first + nreq;
+      ++waves;  // kept in registers: a read of host memory costs a PCIe round trip
+      ops += nops;
+      *(volatile uint64_t*)&j.ctl->waves = waves;
+      *(volatile uint64_t*)&j.ctl->ops = ops;
       st_release_sys_u64(&j.ctl->completed, head);
     }
   }
@@ -996,7 +1052,6 @@ struct lsb_server {
   uint8_t* d_types = nullptr;  // HBM working copy of a wave
   uint64_t* d_keys = nullptr;
   uint64_t* d_vals = nullptr;
-  lsb_result* d_out = nullptr;
   WaveDesc* d_wave = nullptr;
   cudaStream_t stream = nullptr;
   bool running = false;
@@ -1016,7 +1071,6 @@ struct lsb_server {
     cudaFree(d_types);
     cudaFree(d_keys);
     cudaFree(d_vals);
-    cudaFree(d_out);
     cudaFree(d_wave);
   }
 };
@@ -1361,7 +1415,6 @@ int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out)
       cudaMalloc(&s->d_types, wave) == cudaSuccess &&
       cudaMalloc(&s->d_keys, 8ull * wave) == cudaSuccess &&
       cudaMalloc(&s->d_vals, 8ull * wave) == cudaSuccess &&
-      cudaMalloc(&s->d_out, sizeof(lsb_result) * (size_t)wave) == cudaSuccess &&
       cudaMalloc(&s->d_wave, sizeof(WaveDesc)) == cudaSuccess &&
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
   cudaSetDevice(prev);
@@ -1399,7 +1452,6 @@ int lsb_serve_start(lsb_server* s) {
   j.d_types = s->d_types;
   j.d_keys = s->d_keys;
   j.d_vals = s->d_vals;
-  j.d_out = s->d_out;
   j.wave = s->d_wave;
   j.max_wave_ops = s->max_wave_ops;
   j.idle_polls = s->idle_polls;
@@ -1408,7 +1460,7 @@ int lsb_serve_start(lsb_server* s) {
     return LSB_ERR_CUDA;
   }
   FusedJob<MapTraits>& fj = j.fj;
-  fj.base = tb.window(s->d_types, 0, s->d_keys, 1, s->d_vals, 1, s->d_out, kOutResult,
+  fj.base = tb.window(s->d_types, 0, s->d_keys, 1, s->d_vals, 1, j.a_out, kOutResult,
                       s->max_wave_ops);
   fj.window = tb.sc.max_window;
   fj.fused_epoch = tb.fused_epoch;
@@ -1466,8 +1518,13 @@ int lsb_serve_submit(lsb_server* s, const uint8_t* types, const uint64_t* keys,
   std::lock_guard<std::mutex> lk(s->submit_mu);
   const uint64_t freed_req = s->freed_req.load(std::memory_order_acquire);
   const uint64_t freed_op = s->freed_op.load(std::memory_order_acquire);
-  if (s->next_req - freed_req >= s->ring_cap || s->next_op + n - freed_op > s->arena_cap)
+  // a request never wraps the arena's end (a wave's ops stay contiguous):
+  // skip to the next lap when it would
+  uint64_t at = s->next_op;
+  if (at % s->arena_cap + n > s->arena_cap) at += s->arena_cap - at % s->arena_cap;
+  if (s->next_req - freed_req >= s->ring_cap || at + n - freed_op > s->arena_cap)
     return LSB_ERR_STATE;  // full: take results, then retry
+  s->next_op = at;
   uint32_t puts = 0;
   for (uint32_t i = 0; i < n; ++i) {
     const uint64_t pos = (s->next_op + i) % s->arena_cap;

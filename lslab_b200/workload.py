@@ -167,3 +167,19 @@ def set_prefill_keys(seed: int, count: int) -> np.ndarray:
     k = (splitmix64(seed + S_PREFILL, 0, count) >> np.uint64(32)).astype(np.uint32)
     _, first = np.unique(k, return_index=True)
     return k[np.sort(first)]
+
+
+def serving_pool(seed: int, count: int, max_ops: int = 4096, n_items: int = 1 << 28,
+                 theta: float = 0.99, put_frac: float = 0.5):
+    """A pool of serving requests: sizes uniform in [1, max_ops], ops get/put
+    with probability 1 - put_frac / put_frac in arrival order, keys Zipf(theta)
+    over n_items keys, put values uniform u64.  Returns (pool_off, pool_n,
+    types, keys, vals) with each request's ops contiguous."""
+    u = uniform01(seed + S_SIZES, 0, count)
+    n = np.minimum((u * max_ops).astype(np.int64) + 1, max_ops).astype(np.uint32)
+    off = np.concatenate([[0], np.cumsum(n.astype(np.uint64))[:-1]]).astype(np.uint64)
+    total = int(n.astype(np.uint64).sum())
+    types = (uniform01(seed + S_TYPES, 0, total) < put_frac).astype(np.uint8)
+    keys = key_of_rank(seed, zipf_ranks(n_items, theta, seed + S_ZIPF, 0, total))
+    vals = splitmix64(seed + S_VALUES, 0, total)
+    return off, n, types, keys, vals

@@ -177,3 +177,31 @@ def test_serve_ends_after_idle_limit(cuda):
     srv.close()
     assert stats["state"] == 3 and stats["requests"] == 1
     assert m.status() == 0
+
+
+def test_serve_small_arena_wraps_many_laps(cuda):
+    """An arena of 4096 ops and requests of up to 600: requests skip to the
+    next lap instead of wrapping, waves stop at a lap boundary, and slots are
+    reused many times; results still equal the replay."""
+    pool = _requests(13, 64, 600, key_space=300)
+    pool_n = np.array([len(r[1]) for r in pool], np.uint32)
+    pool_off = np.concatenate([[0], np.cumsum(pool_n)[:-1]]).astype(np.uint64)
+    t = np.concatenate([r[0] for r in pool])
+    k = np.concatenate([r[1] for r in pool])
+    v = np.concatenate([r[2] for r in pool])
+    rng = np.random.default_rng(2)
+    nreq = 600
+    idx = rng.integers(0, len(pool), size=nreq).astype(np.uint32)
+    arrival = np.zeros(nreq, np.uint64)  # all due at once: the queue stays full
+    m = Map(8, max_window=1 << 14)
+    srv = Server(m, max_wave_ops=1 << 12, ring_requests=32, arena_ops=1 << 12)
+    srv.start()
+    lat, wall, res = srv.run_load(arrival, idx, pool_off, pool_n, t, k, v, want_results=True)
+    stats = srv.stop()
+    srv.close()
+    assert stats["requests"] == nreq and stats["ops"] == int(pool_n[idx].sum())
+    seq = [slice(int(pool_off[i]), int(pool_off[i]) + int(pool_n[i])) for i in idx]
+    want = OracleMap(8).mixed(np.concatenate([t[s] for s in seq]), np.concatenate([k[s] for s in seq]),
+                              np.concatenate([v[s] for s in seq]))
+    assert same_results(res, want), first_mismatch(res, want)
+    assert m.status() == 0
