@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--serve-loads", default="0.1,0.3,0.5,0.7,0.9,1.0",
                     help="serving: offered loads as fractions of the measured peak")
     ap.add_argument("--nbatches", type=int, default=4096)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batches: use the --block/--chunk/--prefetch tuning instead of the autotuner")
     ap.add_argument("--buckets-log2", type=int, default=22)
     ap.add_argument("--prefill-log2", type=int, default=26)
     ap.add_argument("--batch-log2", type=int, default=20)
@@ -614,7 +616,12 @@ def run_batches(args, world, rank, local):
     # autotune on a sample (the first 256 batches); the plain table gets the
     # sample once as well, so both tables stay identical
     ns = int(sum(sizes[:256]))
-    tuned = fused.autotune(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
+    if args.no_autotune:
+        apply_tuning(args, fused)
+        fused.execute_fused(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
+        tuned = fused.tuning()
+    else:
+        tuned = fused.autotune(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
     plain.execute(d_types[:ns], d_keys[:ns], d_vals[:ns], out_f[:ns])
     graph = fused.capture_fused(d_types, d_keys, d_vals, out_f)
     offs = np.concatenate([[0], np.cumsum(sizes)])

@@ -46,7 +46,7 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 template <class Tr, bool kGroup, int P>
 __global__ void __launch_bounds__(1024, 1)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warp = spread_warp();
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
 }
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, Grid
 template <class Tr>
 __global__ void __launch_bounds__(1024, 1)
     k_resolve(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
   phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
   phase_resolve_reads<Tr>(sc, w, tid, nt);
   release_counters(sc.cnt, bar, nullptr, 0);
@@ -112,7 +112,8 @@ template <class Tr, int P>
 __device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
                               GridBarrier* bar, uint32_t* smem, uint32_t& seq) {
   const uint32_t nblocks = gridDim.x;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  // spread indices: small windows use many SMs; tid 0 is still thread 0 of block 0
+  const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
   const uint32_t warp = tid >> 5, nwarps = nt >> 5;
   const uint32_t nwin = (job.base.n + job.window - 1) / job.window;
   uint32_t tat = 0;
@@ -186,13 +187,24 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     }
     trace_mark(job.trace, tat, wi, 2);
     if (has_mut) {
-      // mutations and later reads resolve independently: half the grid each,
-      // so a small window pays one latency chain instead of two
-      const uint32_t half = (nt / 64) * 32;
-      if (tid < half)
-        phase_resolve_mutations<Tr>(t, sc, w, tid, half);
-      else
-        phase_resolve_reads<Tr>(sc, w, tid - half, nt - half);
+      // Mutations and the reads after the first mutation resolve
+      // independently.  A small window (every thread holds at most one item
+      // of each kind) runs them side by side on two shares of the grid, so
+      // it pays one latency chain instead of two; a large one runs them one
+      // after the other on the whole grid (mutations cost more per item).
+      const uint64_t m = ld_cg_u32(&w.cnt->mut_count);
+      const uint32_t first = ~ld_cg_u32(&w.cnt->inv_first_mut);
+      const uint64_t r = first < w.n ? w.n - first - 1 : 0;
+      const uint32_t ms = (uint32_t)((m + 31) / 32 * 32);
+      if (m + r + 32 <= nt) {
+        if (tid < ms)
+          phase_resolve_mutations<Tr>(t, sc, w, tid, ms);
+        else
+          phase_resolve_reads<Tr>(sc, w, tid - ms, nt - ms);
+      } else {
+        phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
+        phase_resolve_reads<Tr>(sc, w, tid, nt);
+      }
     }
     // Before the next window: its probes must see this window's writes, and
     // its first thread resets this window's counter set, which every block
@@ -377,7 +389,8 @@ template <int P>
 __global__ void __launch_bounds__(1024, 1)
     k_serve(TableView t, Scratch sc, ServeJob j, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  // spread indices (tid < 32 is still warp 0 of block 0)
+  const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
   uint32_t seq = 0;
   uint64_t head = 0;  // meaningful in warp 0 of block 0
   uint64_t waves = 0, ops = 0;  // meaningful in thread 0

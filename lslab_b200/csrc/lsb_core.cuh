@@ -214,6 +214,18 @@ __device__ __forceinline__ uint32_t sm_id() {
 }
 #endif  // LSB_HOST_EMU
 
+// Grid-wide warp index with consecutive warps in different blocks (warp w
+// of block b is number w * gridDim.x + b), and the matching thread index
+// (lanes stay consecutive, so a warp's 32 items stay contiguous).  A grid-
+// stride loop over a small range then spreads over many SMs instead of
+// filling the first few blocks.
+__device__ __forceinline__ uint32_t spread_warp() {
+  return (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
+}
+__device__ __forceinline__ uint32_t spread_tid() {
+  return (threadIdx.x & 31u) + 32u * spread_warp();
+}
+
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bits) {
   atomicOr(status, bits);
 }
