@@ -55,7 +55,7 @@ def parse():
                          "one graph-captured fused launch vs per-op-type calls; serving: the "
                          "request loop under open-loop Poisson load")
     ap.add_argument("--wave-ops", type=int, default=1 << 16, help="serving: ops per wave")
-    ap.add_argument("--serve-seconds", type=float, default=0.4,
+    ap.add_argument("--serve-seconds", type=float, default=1.0,
                     help="serving: offered-load duration of each sweep point")
     ap.add_argument("--serve-loads", default="0.1,0.3,0.5,0.7,0.9,1.0",
                     help="serving: offered loads as fractions of the measured peak")

@@ -256,7 +256,7 @@ struct WaveDesc {     // device: the wave that thread 0 admitted
   uint32_t nreq;       // requests completed by this wave
   uint32_t nops;       // ops run (0 when the head request was refused)
   uint32_t stop;       // 1 drained after a stop request, 2 idle limit
-  uint32_t pad;
+  uint32_t puts;       // puts admitted (worst-case new slabs of the wave)
 };
 
 struct ServeJob {
@@ -271,7 +271,7 @@ struct ServeJob {
   uint8_t* d_types;         // HBM working copy of a wave's ops
   uint64_t* d_keys;
   uint64_t* d_vals;
-  WaveDesc* wave;
+  WaveDesc* wave;           // two descriptors, alternating by admission
   uint32_t max_wave_ops;
   uint32_t idle_polls;
   FusedJob<MapTraits> fj;   // engine parameters; base is set per wave
@@ -293,8 +293,11 @@ __device__ __forceinline__ void st_release_sys_u64(uint64_t* p, uint64_t v) {
 // worst-case new slabs (one per put) fit the pool's free slabs.  Lanes read
 // 32 descriptors at a time and admit by warp prefix sums.  A head request
 // that can never fit the pool (slabs are not returned) is refused alone with
-// LSB_ERR_OOM.
-__device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head) {
+// LSB_ERR_OOM.  `blocking`: wait (bounded) for a request; otherwise an empty
+// queue gives an empty wave.  `in_flight_puts`: puts of a wave still being
+// applied, whose slabs the pool cursor may not show yet.
+__device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out, uint64_t head,
+                            bool blocking, uint64_t in_flight_puts) {
   const uint32_t lane = threadIdx.x & 31;
   WaveDesc wd{};
   wd.first = head;
@@ -303,7 +306,7 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head
   if (lane == 0) {
     for (uint32_t it = 0;; ++it) {
       sub = ld_acquire_sys_u64(&j.ctl->submitted);
-      if (sub > head) break;
+      if (sub > head || !blocking) break;
       if (*(volatile uint32_t*)&j.ctl->stop) {
         stop = 1;
         break;
@@ -317,19 +320,20 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head
   }
   sub = __shfl_sync(0xFFFFFFFFu, sub, 0);
   stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
-  if (stop) {
+  if (stop || sub <= head) {  // stop, or nothing queued (non-blocking)
     if (lane == 0) {
       wd.stop = stop;
-      *j.wave = wd;
+      *out = wd;
     }
     return;
   }
   uint64_t budget = 0;
   if (lane == 0) {
     const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
-    budget = limit > cursor ? limit - cursor : 0;
+    budget = limit > cursor + in_flight_puts ? limit - cursor - in_flight_puts : 0;
   }
   budget = __shfl_sync(0xFFFFFFFFu, budget, 0);
+  const uint64_t budget0 = budget;
   const uint64_t end = min(sub, head + j.ring_cap);
   uint32_t nops = 0, nreq = 0;
   uint64_t next_off = 0;
@@ -364,7 +368,7 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head
         wd.op_off = off;
         wd.nreq = 1;
         wd.nops = 0;
-        *j.wave = wd;
+        *out = wd;
       }
       if (nreq == 0) {
         if (__shfl_sync(0xFFFFFFFFu, valid && puts > budget, 0)) return;
@@ -381,7 +385,9 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, uint64_t head
   if (lane == 0) {
     wd.nreq = nreq;
     wd.nops = nops;
-    *j.wave = wd;
+    const uint64_t used = budget0 - budget;
+    wd.puts = used > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)used;
+    *out = wd;
   }
 }
 
@@ -400,12 +406,19 @@ __global__ void __launch_bounds__(1024, 1)
     ops = *(volatile uint64_t*)&j.ctl->ops;
   }
   if (tid == 0) *(volatile uint32_t*)&j.ctl->state = 1;
+  // Wave k+1 is admitted (without waiting) as wave k's last phase ends, so
+  // one grid barrier both completes wave k and publishes wave k+1; only an
+  // empty queue makes warp 0 wait for requests, after wave k is published.
+  // Admission `a` writes descriptor a & 1, which every block finished
+  // reading before the barrier of admission a - 1.
+  uint32_t a = 0;
+  if (tid < 32) serve_admit(t, j, &j.wave[0], head, true, 0);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) goto out;
   for (;;) {
-    if (tid < 32) serve_admit(t, j, head);
-    if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
-    const uint64_t first = ld_cg_u64(&j.wave->first), op_off = ld_cg_u64(&j.wave->op_off);
-    const uint32_t nreq = ld_cg_u32(&j.wave->nreq), nops = ld_cg_u32(&j.wave->nops);
-    const uint32_t stop = ld_cg_u32(&j.wave->stop);
+    const WaveDesc* cur = &j.wave[a & 1];
+    const uint64_t first = ld_cg_u64(&cur->first), op_off = ld_cg_u64(&cur->op_off);
+    const uint32_t nreq = ld_cg_u32(&cur->nreq), nops = ld_cg_u32(&cur->nops);
+    const uint32_t stop = ld_cg_u32(&cur->stop), wave_puts = ld_cg_u32(&cur->puts);
     if (stop) {
       if (tid == 0) *(volatile uint32_t*)&j.ctl->state = stop == 1 ? 2 : 3;
       break;
@@ -431,9 +444,11 @@ __global__ void __launch_bounds__(1024, 1)
       fj.base.out = j.a_out + pos;  // results go straight to the host-mapped arena
       fj.base.n = nops;
       fused_windows<MapTraits, P>(t, sc, fj, bar, smem, seq);
-      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     }
-    if (tid < 32) head = first + nreq;
+    const uint64_t next = first + nreq;
+    ++a;
+    if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, false, wave_puts);
+    if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     if (tid == 0) {
       win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
       __threadfence_system();          // results before the completion count
@@ -441,9 +456,16 @@ __global__ void __launch_bounds__(1024, 1)
       ops += nops;
       *(volatile uint64_t*)&j.ctl->waves = waves;
       *(volatile uint64_t*)&j.ctl->ops = ops;
-      st_release_sys_u64(&j.ctl->completed, head);
+      st_release_sys_u64(&j.ctl->completed, next);
+    }
+    if (ld_cg_u32(&j.wave[a & 1].nreq) == 0 && ld_cg_u32(&j.wave[a & 1].stop) == 0) {
+      // the queue was empty: wait for requests now that wave k is published
+      ++a;
+      if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, true, 0);
+      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     }
   }
+out:
   if (tid == 0 && (*(volatile uint32_t*)t.status & kStatusBarrier))
     *(volatile uint32_t*)&j.ctl->state = 4;
   release_counters(sc.cnt, bar, j.fj.bins, 2 * sizeof(BinCounters) / 4);
@@ -1428,7 +1450,7 @@ int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out)
       cudaMalloc(&s->d_types, wave) == cudaSuccess &&
       cudaMalloc(&s->d_keys, 8ull * wave) == cudaSuccess &&
       cudaMalloc(&s->d_vals, 8ull * wave) == cudaSuccess &&
-      cudaMalloc(&s->d_wave, sizeof(WaveDesc)) == cudaSuccess &&
+      cudaMalloc(&s->d_wave, 2 * sizeof(WaveDesc)) == cudaSuccess &&
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
   cudaSetDevice(prev);
   if (!ok) {

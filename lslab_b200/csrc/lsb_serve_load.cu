@@ -4,6 +4,9 @@
 // records each request's latency from its scheduled arrival, so queueing
 // delay on the host (a full queue) counts against latency as it would for a
 // real client.
+#include <pthread.h>
+#include <sched.h>
+
 #include <atomic>
 #include <chrono>
 #include <thread>
@@ -16,6 +19,24 @@ using Clock = std::chrono::steady_clock;
 
 // longest wait for one request before the run is abandoned
 constexpr uint64_t kWaitLimitNs = 30ull * 1000 * 1000 * 1000;
+
+// The two busy threads each get a core of their own (the last two CPUs the
+// process may use), so a scheduler migration does not stall a request.
+inline void pin_to(int nth_from_last) {
+  cpu_set_t set;
+  if (sched_getaffinity(0, sizeof(set), &set) != 0) return;
+  int seen = 0;
+  for (int c = CPU_SETSIZE - 1; c >= 0; --c) {
+    if (!CPU_ISSET(c, &set)) continue;
+    if (seen++ == nth_from_last) {
+      cpu_set_t one;
+      CPU_ZERO(&one);
+      CPU_SET(c, &one);
+      pthread_setaffinity_np(pthread_self(), sizeof(one), &one);
+      return;
+    }
+  }
+}
 
 inline uint64_t ns_since(Clock::time_point t0) {
   return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - t0).count();
@@ -45,7 +66,10 @@ extern "C" int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* ld, uint6
   std::atomic<int> error{LSB_OK};
   const Clock::time_point t0 = Clock::now();
 
+  cpu_set_t saved;
+  const bool have_saved = pthread_getaffinity_np(pthread_self(), sizeof(saved), &saved) == 0;
   std::thread taker([&] {
+    pin_to(1);
     for (uint64_t i = 0; i < nreq; ++i) {
       while (issued.load(std::memory_order_acquire) <= i) {
         if (error.load() != LSB_OK) return;
@@ -74,6 +98,7 @@ extern "C" int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* ld, uint6
     }
   });
 
+  pin_to(0);
   for (uint64_t i = 0; i < nreq && error.load() == LSB_OK; ++i) {
     while (ns_since(t0) < ld->arrival_ns[i]) {
     }
@@ -96,5 +121,6 @@ extern "C" int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* ld, uint6
   }
   taker.join();
   if (wall_ns) *wall_ns = ns_since(t0);
+  if (have_saved) pthread_setaffinity_np(pthread_self(), sizeof(saved), &saved);
   return error.load();
 }
