@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="zipf9505", choices=["zipf9505", "batches", "serving"],
+    ap.add_argument("--workload", default="zipf9505",
+                    choices=["zipf9505", "batches", "serving", "sets", "locks"],
                     help="zipf9505: the headline line; batches: 4096 uneven mixed batches in "
                          "one graph-captured fused launch vs per-op-type calls; serving: the "
                          "request loop under open-loop Poisson load")
@@ -748,6 +749,149 @@ def run_serving(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def _perm32(torch, idx):
+    """Distinct u32 keys on the device: a bijective 32-bit mix of `idx`
+    (odd multiplies and xor-shifts modulo 2^32), as int32 tensors."""
+    m = 0xFFFFFFFF
+    x = idx.to(torch.int64) & m
+    x = ((x ^ (x >> 16)) * 0x7FEB352D) & m
+    x = ((x ^ (x >> 15)) * 0x846CA68B) & m
+    x = x ^ (x >> 16)
+    return (x - ((x >> 31) << 32)).to(torch.int32)  # two's-complement view
+
+
+def run_sets(args, world, rank, local):
+    """Set load-factor sweep: set<u32> with 2^18 buckets (42 MB of head slabs,
+    L2-resident) and 2^22 buckets (671 MB of heads plus the chains the load
+    needs, HBM-resident), prefilled to 0.25 .. 4 keys per head-slab slot;
+    batches of 2^18 ops, 40% insert / 50% contains / 10% remove over a
+    universe of the prefill keys and as many absent keys (uniform).  Fused:
+    one execute_fused per batch; plain: per batch the insert, contains and
+    remove calls of its type-sorted parts."""
+    import torch
+    import lslab_b200 as L
+    from lslab_b200.shard import rank_seed
+
+    seed = rank_seed(args.seed, rank)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    n = 1 << 18
+    points = []
+    for log2 in (18, 22):
+        for lf in (0.25, 0.5, 1.0, 2.0, 4.0):
+            nk = int(lf * (1 << log2) * 28)
+            pool = max(4096, int(nk / 28 * 1.5) + (1 << log2) // 4)
+            res = {}
+            for form in ("fused", "plain"):
+                st = L.Set(log2, pool)
+                for off in range(0, nk, 1 << 24):
+                    k = _perm32(torch, torch.arange(off, min(nk, off + (1 << 24)), device="cuda"))
+                    st.insert(k)
+                    del k
+                torch.cuda.synchronize()
+                gen.manual_seed(seed + log2 * 100 + int(lf * 8))
+                nb = args.warmup + args.steps
+                batches = []
+                for _ in range(nb):
+                    u = torch.rand(n, device="cuda", generator=gen)
+                    ty = torch.where(u < 0.4, 1, torch.where(u < 0.9, 0, 2)).to(torch.uint8)
+                    ty, _ = torch.sort(ty)  # contains, insert, remove: type-sorted parts
+                    idx = torch.randint(0, 2 * nk, (n,), device="cuda", generator=gen)
+                    batches.append((ty, _perm32(torch, idx)))
+                out = torch.empty(n, dtype=torch.bool, device="cuda")
+                cnt = [(int((b[0] == 0).sum()), int((b[0] == 1).sum())) for b in batches]
+
+                def step(i):
+                    ty, k = batches[i]
+                    if form == "fused":
+                        st.execute_fused(ty, k, out)
+                    else:
+                        c, ins = cnt[i]
+                        if c:
+                            st.contains(k[:c], out[:c])
+                        if ins:
+                            st.insert(k[c:c + ins], out[c:c + ins])
+                        if n - c - ins:
+                            st.remove(k[c + ins:], out[c + ins:])
+                for i in range(args.warmup):
+                    step(i)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for i in range(args.warmup, nb):
+                    step(i)
+                e1.record()
+                torch.cuda.synchronize()
+                res[form] = round(args.steps * n / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)
+                res["status"] = res.get("status", 0) | st.status()
+                st.close()
+                del batches
+            points.append({"buckets_log2": log2, "keys_per_slot": lf, "keys": nk,
+                           "head_mb": round((1 << log2) * 160 / 1e6, 1),
+                           "fused_mops": res["fused"], "plain_mops": res["plain"],
+                           "device_status": res["status"]})
+    if rank == 0:
+        print(json.dumps({"workload": "sets", "description": run_sets.__doc__.split(".")[0],
+                          "batch_ops": n, "steps": args.steps, "points": points}), flush=True)
+
+
+def run_locks(args, world, rank, local):
+    """Bucket-lock comparison on the map (writer lock = the reference's
+    warp_mutex role; lock-free = CAS on slab tag words; rw = reader-writer
+    locks on the read path too): 2^20-op batches, Zipf 0.99 over 2^26 keys on
+    2^22 buckets prefilled with 2^26 keys, 95/5 and 50/50 get/put, fused and
+    per-op-type forms.  Results are identical across modes (tests)."""
+    import torch
+    import lslab_b200 as L
+
+    n = 1 << args.batch_log2
+    nb = args.warmup + args.steps
+    pk, pv = prefill_arrays(args, rank)
+    pool = max(1 << (args.buckets_log2 - 2), 4096)
+    rows = []
+    for put_frac in (0.05, 0.5):
+        args.put_frac = put_frac
+        batches = make_batches(args, rank, nb)
+        dT = [torch.from_numpy(b.types).cuda() for b in batches]
+        dK = [dev_u64(torch, b.keys) for b in batches]
+        dV = [dev_u64(torch, b.vals) for b in batches]
+        ng = [int(np.sum(b.types == 0)) for b in batches]
+        out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+        old = torch.empty(n, dtype=torch.int64, device="cuda")
+        for mode in ("writer", "free", "rw"):
+            m = L.Map(args.buckets_log2, pool, lock_mode=mode)
+            for off in range(0, len(pk), 1 << 24):
+                k = dev_u64(torch, pk[off:off + (1 << 24)])
+                v = dev_u64(torch, pv[off:off + (1 << 24)])
+                m.put(k, v)
+                del k, v
+            row = {"put_frac": put_frac, "lock_mode": mode}
+            for form in ("fused", "plain"):
+                def step(i):
+                    if form == "fused":
+                        m.execute_fused(dT[i], dK[i], dV[i], out)
+                    else:
+                        g = ng[i]
+                        m.get(dK[i][:g], out[:g])
+                        m.put(dK[i][g:], dV[i][g:], old[g:])
+                for i in range(args.warmup):
+                    step(i)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for i in range(args.warmup, nb):
+                    step(i)
+                e1.record()
+                torch.cuda.synchronize()
+                row[form + "_mops"] = round(args.steps * n / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)
+            row["device_status"] = m.status()
+            m.close()
+            rows.append(row)
+    if rank == 0:
+        print(json.dumps({"workload": "locks", "description": run_locks.__doc__.split(".")[0],
+                          "rows": rows}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -757,6 +901,10 @@ def main():
         run_batches(args, world, rank, local)
     elif args.workload == "serving":
         run_serving(args, world, rank, local)
+    elif args.workload == "sets":
+        run_sets(args, world, rank, local)
+    elif args.workload == "locks":
+        run_locks(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
     if world > 1:

@@ -309,31 +309,33 @@ constexpr uint32_t kPoolChunkMax = 32;
 
 // ------------------------------------------------------------ slab pool
 // Per-SM bump ranges refilled in chunks from one global cursor.  A range is
-// one u64 {end:32 | cur:32}; atomicAdd on it hands out cur.  When a range is
-// spent the thread takes a fresh chunk from the global cursor and installs
-// it; if two threads refill the same SM at once the later install wins and
-// the rest of the earlier chunk is never handed out (at most chunk - 1 slabs
-// per race).  The chunk shrinks with the pool (down to 1 slab, i.e. a plain
-// global bump) so that per-SM ranges cannot strand a small pool.  Pool memory is zeroed at creation and slabs are never
-// returned, so a slab is always empty when handed out.  Replaces the
-// reference's single global fetch_add with __trap on overflow
+// one u64 {end:32 | cur:32}; atomicAdd on it hands out cur.  Exactly one
+// thread sees cur == end when a range is spent: it takes a fresh chunk from
+// the global cursor and installs it.  Threads that arrive while it does so
+// (cur > end) take single slabs from the global cursor, so no chunk is ever
+// abandoned half used.  The chunk shrinks with the pool (down to 1 slab,
+// i.e. a plain global bump).  Pool memory is zeroed at creation and slabs
+// are never returned, so a slab is always empty when handed out.  Replaces
+// the reference's single global fetch_add with __trap on overflow
 // (include/lslab/detail/device_allocator.h:63-70): here exhaustion returns 0
 // and raises kStatusOOM.
 __device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
   const uint32_t smid = sm_id();
   unsigned long long* range = (unsigned long long*)&t.pool[2 + (smid & (kPoolSlots - 1))];
-  unsigned long long old = atomicAdd(range, 1ull);
-  uint32_t cur = (uint32_t)old, end = (uint32_t)(old >> 32);
+  const unsigned long long old = atomicAdd(range, 1ull);
+  const uint32_t cur = (uint32_t)old, end = (uint32_t)(old >> 32);
   if (cur < end) return cur;
-  unsigned long long base = atomicAdd((unsigned long long*)&t.pool[0], (unsigned long long)t.chunk);
-  unsigned long long limit = t.pool[1];
+  const unsigned long long limit = t.pool[1];
+  const unsigned long long take = cur == end ? t.chunk : 1ull;  // refill, or a single slab
+  const unsigned long long base = atomicAdd((unsigned long long*)&t.pool[0], take);
   if (base >= limit) {
     raise_status(t.status, kStatusOOM);
     return 0;
   }
-  unsigned long long stop = base + t.chunk;
-  if (stop > limit) stop = limit;
-  if (base + 1 < stop) atomicExch(range, (stop << 32) | (base + 1));
+  if (cur == end) {
+    const unsigned long long stop = base + take < limit ? base + take : limit;
+    atomicExch(range, (stop << 32) | (base + 1));  // base + 1 == stop: spent again
+  }
   return (uint32_t)base;
 }
 

@@ -9,6 +9,7 @@
 // Atomics are GCC __atomic builtins on host memory.
 #pragma once
 
+#include <atomic>
 #include <barrier>
 #include <cassert>
 #include <cstdint>
@@ -45,6 +46,7 @@ struct Block {
   std::unique_ptr<std::barrier<>> bar;
   std::vector<std::unique_ptr<std::barrier<>>> warp_bar;
   std::vector<uint64_t> buf;  // 32 words per warp
+  std::atomic<int> or_flag{0};  // __syncthreads_or
 };
 
 inline thread_local Block* blk = nullptr;
@@ -92,6 +94,16 @@ void run_block(unsigned nthreads, unsigned block, unsigned nblocks, F&& f) {
 }  // namespace emu
 
 inline void __syncthreads() { emu::blk->bar->arrive_and_wait(); }
+inline int __syncthreads_or(int pred) {
+  emu::Block* b = emu::blk;
+  if (pred) b->or_flag.store(1);
+  b->bar->arrive_and_wait();
+  const int r = b->or_flag.load();
+  b->bar->arrive_and_wait();
+  if (threadIdx.x == 0) b->or_flag.store(0);
+  b->bar->arrive_and_wait();
+  return r;
+}
 inline void __threadfence() { __atomic_thread_fence(__ATOMIC_SEQ_CST); }
 inline void __threadfence_block() { __atomic_thread_fence(__ATOMIC_SEQ_CST); }
 inline void __nanosleep(unsigned) { std::this_thread::yield(); }

@@ -84,3 +84,26 @@ def test_set_batches_per_type_vs_oracle(cuda):
         assert np.array_equal(got, want)
     assert np.array_equal(s.dump(), o.dump())
     assert s.status() == 0
+
+
+def test_pool_not_wasted_by_concurrent_inserts(cuda):
+    """Two keys per head slot inserted in large batches: chains need about one
+    overflow slab per bucket, and concurrent refills of a per-SM slab range
+    must not abandon half-used chunks (the pool then runs out)."""
+    import torch
+    from lslab_b200 import Set
+    log2 = 14
+    buckets = 1 << log2
+    nk = 2 * buckets * 28
+    pool = int(1.55 * buckets) + 148 * 32
+    s = Set(log2, pool)
+    keys = np.unique(W.splitmix64(91, 0, 2 * nk).astype(np.uint32))[:nk]
+    for off in range(0, nk, 1 << 18):
+        s.insert(torch.from_numpy(keys[off:off + (1 << 18)].view(np.int32)).cuda())
+    torch.cuda.synchronize()
+    used, cap = s.pool_usage()
+    assert s.status() == 0
+    assert s.size() == len(keys)
+    # Poisson(56) keys per bucket need ~1.47 overflow slabs per bucket; each
+    # SM may hold one partly used chunk (at most 32 slabs) on top
+    assert used <= int(1.55 * buckets) + 148 * 32, (used, buckets)
