@@ -236,7 +236,8 @@ int lsb_set_dump(lsb_set* s, uint32_t* keys_out, size_t cap, uint64_t* count,
 typedef struct lsb_graph lsb_graph;
 
 /* Capture lsb_map_execute_fused on these buffers into an instantiated CUDA
- * graph (one memset and one cooperative kernel).  Each lsb_graph_launch runs
+ * graph (one cooperative kernel; its counters are left zero by the previous
+ * launch, so no memset precedes it).  Each lsb_graph_launch runs
  * the batch currently in the buffers; the window epochs live on the device,
  * so replays never reuse one. */
 int lsb_map_capture_fused(lsb_map* m, const uint8_t* types, const uint64_t* keys,
