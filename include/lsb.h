@@ -92,7 +92,9 @@ typedef struct lsb_tuning {
   uint32_t prefetch;      /* extra lookups a thread keeps in flight: 0, 1 or 2 */
   uint32_t dedup;         /* 1: lanes of a warp carrying the same key share one lookup */
   uint32_t fused_split;   /* fused path: percent of a window's reads probed before the
-                             same-key ordering pass (the rest run during it), 0..100 */
+                             same-key ordering pass (the rest run during it), 0..100;
+                             0 = the mutations are listed and probed first while blocks
+                             take reads, the remaining reads run during the ordering */
   uint32_t region_order;  /* fused path: 1 = probe a window in table-region order */
 } lsb_tuning;
 
@@ -248,8 +250,10 @@ int lsb_graph_launch(lsb_graph* g, cudaStream_t stream);
 int lsb_graph_destroy(lsb_graph* g);
 
 /* Autotuner: times the fused path on a sample batch for every block size
- * (256, 512, 1024 threads = 8, 16, 32 warps), probe claim size (static, 1024,
- * 2048, 4096 ops) and lookahead (0, 1, 2), keeps the fastest on the table
+ * (256, 512, 1024 threads = 8, 16, 32 warps), lookahead (0, 1, 2) and probe
+ * order (mutations listed and probed first, reads meanwhile and after; or
+ * all ops in one pass with claim size static, 1024, 2048 or 4096 ops),
+ * keeps the fastest on the table
  * and in a process-wide cache by table size that tables created later with
  * the same log2_buckets start from.  The sample is applied once per
  * candidate: the final table contents equal one application (a key's final

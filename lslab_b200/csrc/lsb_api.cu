@@ -146,19 +146,39 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     if (tid == 0) win_counters_reset(&sc.cnt[(wi + 1) & 1]);
     if (tid < 2 * kBins) (&job.bins[(wi + 1) & 1].count[0])[tid] = 0;
     const uint32_t* perm = nullptr;
-    if (job.binned) {
-      phase_bin_count<Tr>(t, w, sc.obin, &job.bins[wi & 1], job.bin_shift);
-      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
-      phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
-      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
-      perm = sc.perm;
-    }
     // Reads [0, split) are probed with the mutations; reads [split, n) in the
     // sort pass, where they fill the SMs that the (latency-bound, few-block)
     // ordering of big groups leaves idle.  Reads do not depend on the groups.
     const uint32_t split = (uint32_t)(((uint64_t)w.n * job.split_q16) >> 16);
-    phase_probe<Tr, true, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, job.chunk,
-                             job.dedup != 0, ProbeSel{0, split, true}, 0, perm);
+    if (split == 0) {
+      // Mutations listed, then probed from the list; while their (latency-
+      // bound) chains run, blocks take reads from the same cursor as the sort
+      // pass, until every list tile is done.  Region binning of the reads
+      // rides along the two steps.
+      phase_list_muts<Tr>(sc, w, warp, nwarps);
+      if (job.binned) phase_bin_count<Tr>(t, w, sc.obin, &job.bins[wi & 1], job.bin_shift);
+      if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+      const uint32_t listed = min(ld_cg_u32(&w.cnt->clist_count), clist_cap(sc.max_window));
+      phase_probe_list<Tr>(t, sc, w, warp, nwarps, job.dedup != 0);
+      if (job.binned) {
+        phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
+        perm = sc.perm;
+      } else {
+        phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, blockDim.x * P,
+                                  job.dedup != 0, ProbeSel{0, w.n, false}, 0, nullptr,
+                                  &w.cnt->tiles_done, (listed + 31) / 32);
+      }
+    } else {
+      if (job.binned) {
+        phase_bin_count<Tr>(t, w, sc.obin, &job.bins[wi & 1], job.bin_shift);
+        if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+        phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
+        if (!grid_barrier(bar, nblocks, t.status, seq)) return;
+        perm = sc.perm;
+      }
+      phase_probe<Tr, true, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, job.chunk,
+                               job.dedup != 0, ProbeSel{0, split, true}, 0, perm);
+    }
     if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     // every block has read the epoch counter (before its first barrier)
     if (wi == 0 && tid == 0) *job.fused_epoch = f + nwin;
@@ -552,7 +572,7 @@ struct Table {
   uint32_t chunk = 1;  // per-SM pool refill size
   int num_sms = 0;
   Tuning tune;
-  uint32_t split_q16 = 65536;  // all of a window's reads probed before the sort pass
+  uint32_t split_q16 = 0;  // mutations listed and probed first, reads fill in (fused_split 0)
   uint64_t* trace = nullptr;   // device phase-trace buffer when tracing is on
   BinCounters* bins = nullptr; // inside the counter block (see kCounterBytes)
   uint32_t* fused_epoch = nullptr;  // device counter of fused windows (see k_fused)
@@ -574,7 +594,7 @@ struct Table {
   void release() {
     void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
-                    sc.cnt, sc.obin, sc.perm, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
+                    sc.cnt, sc.obin, sc.perm, sc.clist, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
                     trace, fused_epoch};
     for (void* p : ptrs) cudaFree(p);
   }
@@ -624,6 +644,7 @@ struct Table {
         cudaMalloc(&sc.large, sizeof(uint32_t) * (window / (kWarpSort + 1) + 1)) == cudaSuccess &&
         cudaMalloc(&sc.obin, window) == cudaSuccess &&
         cudaMalloc(&sc.perm, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.clist, sizeof(uint32_t) * clist_cap(window)) == cudaSuccess &&
         cudaMalloc(&sc.hlist, sizeof(uint32_t) * sc.hcap) == cudaSuccess &&
         cudaMalloc(&sc.hrec, sizeof(uint32_t) * 4 * sc.hcap) == cudaSuccess &&
         cudaMalloc(&sc.hbins, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap) == cudaSuccess &&
@@ -977,11 +998,13 @@ int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::K
   int err = LSB_OK;
   for (uint32_t block : {256u, 512u, 1024u}) {
     for (uint32_t prefetch : {0u, 1u, 2u}) {
-      for (uint32_t chunk : {0u, 1024u, 2048u, 4096u}) {
+      // split 0 (mutations listed first) has no claim size to tune
+      for (uint32_t chunk : {0xFFFFFFFFu, 0u, 1024u, 2048u, 4096u}) {
         lsb_tuning c = cur;
         c.block_threads = block;
         c.prefetch = prefetch;
-        c.chunk = chunk;
+        c.chunk = chunk == 0xFFFFFFFFu ? 0u : chunk;
+        c.fused_split = chunk == 0xFFFFFFFFu ? 0u : 100u;
         if (tb.set_tuning(c) != LSB_OK) continue;
         if (tb.fused_grid() <= 0) continue;  // shape cannot be co-resident
         err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);  // warm-up
@@ -1501,7 +1524,7 @@ int lsb_serve_start(lsb_server* s) {
   fj.fused_epoch = tb.fused_epoch;
   fj.chunk = tb.tune.chunk;
   fj.dedup = tb.tune.dedup;
-  fj.split_q16 = tb.split_q16;
+  fj.split_q16 = 65536;  // a wave: every op in one probe pass (one grid barrier fewer)
   fj.trace = nullptr;
   fj.bins = tb.bins;
   fj.binned = 0;

@@ -58,11 +58,11 @@ struct WinCounters {
   uint32_t mut_count;
   uint32_t seg_cursor;
   uint32_t big_count;
-  uint32_t pad0;
+  uint32_t clist_count;    // entries of the compacted mutation list
   uint32_t inv_first_mut;  // ~(lowest mutation index); 0 = no mutation
   uint32_t probe_cursor;   // next op to hand out when the probe claims chunks
   uint32_t large_count;    // groups with more than kWarpSort members
-  uint32_t pad1;
+  uint32_t tiles_done;     // mutation-list tiles probed (reads fill in meanwhile)
   uint32_t late_cursor;    // next late read handed out in the fused sort pass
   uint32_t huge_count;     // groups with more than kHugeMin members
   uint32_t run_count;      // runs of huge groups (each sorted by one block)
@@ -73,10 +73,12 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->mut_count = 0;
   c->seg_cursor = 0;
   c->big_count = 0;
+  c->clist_count = 0;
   c->inv_first_mut = 0;
   c->probe_cursor = 0;
   c->large_count = 0;
   c->late_cursor = 0;
+  c->tiles_done = 0;
   c->huge_count = 0;
   c->run_count = 0;
 }
@@ -111,6 +113,7 @@ struct Scratch {
   uint32_t* runs;   // per run: seg begin, seg end, info, 1 + largest member
   uint32_t hcap;
   uint32_t rcap;
+  uint32_t* clist;  // compacted mutation indices, clist_cap(max_window) entries
   uint32_t* status; // the table's device status word
 };
 
@@ -309,30 +312,21 @@ struct ProbeSel {
   bool muts;
 };
 
-// `perm` (optional): position -> op index (the binned order); positions
-// base + j*32 + lane are then mapped to ops, and sel's read range is in
-// positions.
+// Probe (and, for mutations, group) the ops idx[j] whose type and key the
+// caller loaded; lanes in ascending op-index order.  Every lane of the warp
+// calls it.
 template <class Tr, bool kGroup, int P>
-__device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc,
-                                           const Window<Tr>& w, uint32_t base, uint32_t lane,
-                                           bool dedup, const ProbeSel& sel,
-                                           const uint32_t* perm) {
-  using Key = typename Tr::Key;
+__device__ __forceinline__ void probe_ops(const TableView& t, const Scratch& sc,
+                                          const Window<Tr>& w, uint32_t lane, bool dedup,
+                                          const uint32_t (&idx)[P], const uint8_t (&type)[P],
+                                          const bool (&active)[P],
+                                          const typename Tr::Key (&key)[P]) {
   const uint32_t lanemask_lt = (1u << lane) - 1u;
-  Key key[P];
   uint64_t h[P], value[P], loc[P];
-  uint8_t type[P];
-  bool active[P], want[P], found[P];
-  uint32_t src[P], idx[P];
+  bool want[P], found[P];
+  uint32_t src[P];
 #pragma unroll
   for (int j = 0; j < P; ++j) {
-    const uint32_t pos = base + j * 32 + lane;
-    uint32_t i = pos;
-    if (perm != nullptr && pos < w.n) i = min(ld_cs_u32(perm + pos), w.n);
-    idx[j] = i;
-    type[j] = i < w.n ? (perm ? op_type(w, i) : op_type_stream(w, i)) : kOpRead;
-    active[j] = i < w.n && (type[j] == kOpRead ? (pos >= sel.read_lo && pos < sel.read_hi) : sel.muts);
-    key[j] = active[j] ? (perm ? key_of(w, i) : key_stream(w, i)) : (Key)0;
     h[j] = Tr::hash(key[j]);
     want[j] = active[j];
     src[j] = lane;
@@ -399,18 +393,131 @@ __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc
   }
 }
 
+// Ops base + j*32 + lane, j < P.  `perm` (optional): position -> op index
+// (the binned order); positions are then mapped to ops, and sel's read range
+// is in positions.
+template <class Tr, bool kGroup, int P>
+__device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc,
+                                           const Window<Tr>& w, uint32_t base, uint32_t lane,
+                                           bool dedup, const ProbeSel& sel,
+                                           const uint32_t* perm) {
+  using Key = typename Tr::Key;
+  Key key[P];
+  uint8_t type[P];
+  bool active[P];
+  uint32_t idx[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const uint32_t pos = base + j * 32 + lane;
+    uint32_t i = pos;
+    if (perm != nullptr && pos < w.n) i = min(ld_cs_u32(perm + pos), w.n);
+    idx[j] = i;
+    type[j] = i < w.n ? (perm ? op_type(w, i) : op_type_stream(w, i)) : kOpRead;
+    active[j] = i < w.n && (type[j] == kOpRead ? (pos >= sel.read_lo && pos < sel.read_hi) : sel.muts);
+    key[j] = active[j] ? (perm ? key_of(w, i) : key_stream(w, i)) : (Key)0;
+  }
+  probe_ops<Tr, kGroup, P>(t, sc, w, lane, dedup, idx, type, active, key);
+}
+
+// Phase A for the mutations of a window alone (its reads are probed in a
+// later pass), in two grid steps with a grid barrier between them.
+// Step 1 (phase_list_muts): a warp takes 512-op spans; each lane reads the
+// types of 16 consecutive ops with one 16-byte load, and the span's mutations
+// are appended in op-index order to a list, padded to whole 32-entry tiles
+// (one atomic per span).  Step 2 (phase_probe_list): the tiles are probed and
+// grouped by all warps.  A read-mostly window then costs two short passes
+// instead of one dependent chain per 32 ops, and dense runs of mutations are
+// spread over every warp of the grid.
+constexpr uint32_t kListSpan = 512;
+
+__host__ __device__ constexpr uint32_t clist_cap(uint32_t window) {
+  return window + 32u * (window / kListSpan + 1u);  // each span pads < 32 entries
+}
+
+template <class Tr>
+__device__ void phase_list_muts(const Scratch& sc, const Window<Tr>& w, uint32_t warp_id,
+                                uint32_t num_warps) {
+  constexpr uint32_t kPer = kListSpan / 32;
+  if (w.types == nullptr && w.uniform == kOpRead) return;
+  const uint32_t lane = lane_id();
+  const uint32_t cap = clist_cap(sc.max_window);
+  for (uint32_t base = warp_id * kListSpan; base < w.n; base += num_warps * kListSpan) {
+    const uint32_t o = base + lane * kPer;
+    uint32_t bits = 0;  // bit k: op o + k is a mutation
+    if (w.types == nullptr) {
+      if (o < w.n) bits = w.n - o >= kPer ? 0xFFFFu : (1u << (w.n - o)) - 1u;
+    } else if (((uintptr_t)(w.types + base) & 15u) == 0 && base + kListSpan <= w.n) {
+      // warp-uniform: the span is whole and its lanes' 16 bytes are aligned
+      const uint4 v = ld_cg_v4(w.types + o);
+      const uint32_t word[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (((word[q >> 2] >> (8 * (q & 3))) & 0xFFu) != kOpRead) bits |= 1u << q;
+    } else {
+      for (uint32_t q = 0; q < kPer && o + q < w.n; ++q)
+        if (op_type(w, o + q) != kOpRead) bits |= 1u << q;
+    }
+    const uint32_t c = __popc(bits);
+    uint32_t incl = c;  // inclusive prefix of the lanes' counts
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if (lane >= d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (total == 0) continue;  // warp-uniform
+    const uint32_t padded = (total + 31u) & ~31u;
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(&w.cnt->clist_count, padded);
+    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+    if (at > cap || padded > cap - at) {  // cannot happen: the list is sized for every span
+      if (lane == 0) raise_status(sc.status, kStatusScratch);
+      continue;
+    }
+    uint32_t* dst = sc.clist + at + (incl - c);
+    for (uint32_t m = bits; m; m &= m - 1u) *dst++ = o + (uint32_t)(__ffs(m) - 1);
+    if (lane < padded - total) sc.clist[at + total + lane] = 0xFFFFFFFFu;
+  }
+}
+
+template <class Tr>
+__device__ void phase_probe_list(const TableView& t, const Scratch& sc, const Window<Tr>& w,
+                                 uint32_t warp_id, uint32_t num_warps, bool dedup) {
+  using Key = typename Tr::Key;
+  const uint32_t lane = lane_id();
+  const uint32_t total = min(ld_cg_u32(&w.cnt->clist_count), clist_cap(sc.max_window));
+  for (uint32_t tile = warp_id * 32; tile < total; tile += num_warps * 32) {
+    const uint32_t i = tile + lane < total ? ld_cg_u32(sc.clist + tile + lane) : 0xFFFFFFFFu;
+    uint32_t idx[1] = {0xFFFFFFFFu};
+    uint8_t type[1] = {kOpRead};
+    bool active[1] = {false};
+    Key key[1] = {(Key)0};
+    if (i < w.n) {
+      idx[0] = i;
+      type[0] = op_type(w, i);
+      active[0] = type[0] != kOpRead;
+      key[0] = key_of(w, i);
+    }
+    probe_ops<Tr, true, 1>(t, sc, w, lane, dedup, idx, type, active, key);
+    if (lane == 0) atomicAdd(&w.cnt->tiles_done, 1u);
+  }
+}
+
 // Phase A over the window from op `begin`.  cursor == null or chunk == 0:
 // warp-uniform grid stride of 32*P ops.  Otherwise work is claimed in two
 // levels: a block takes `chunk` consecutive ops with one atomic on *cursor,
 // its warps take 32*P-op tiles of that chunk from a shared counter; blocks
 // that finish early take more chunks (balance without a global atomic per
-// tile).  Every thread of the block must call it.
+// tile).  With `stop_at`, a block takes no further chunk once *stop_at has
+// reached stop_target (the rest is claimed by a later call on the same
+// cursor).  Every thread of the block must call it.
 template <class Tr, bool kGroup, int P>
 __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<Tr>& w,
                             uint32_t warp_id, uint32_t num_warps, uint32_t* cursor,
                             uint32_t chunk, bool dedup,
                             ProbeSel sel = ProbeSel{0, 0xFFFFFFFFu, true}, uint32_t begin = 0,
-                            const uint32_t* perm = nullptr) {
+                            const uint32_t* perm = nullptr, const uint32_t* stop_at = nullptr,
+                            uint32_t stop_target = 0) {
   const uint32_t lane = lane_id();
   if (cursor == nullptr || chunk == 0) {
     for (uint32_t base = begin + warp_id * 32 * P; base < w.n; base += num_warps * 32 * P)
@@ -423,7 +530,10 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
   chunk = max(32u * P, chunk - chunk % (32u * P));
   for (;;) {
     if (threadIdx.x == 0) {
-      s_base = begin + atomicAdd(cursor, chunk);
+      // checked before claiming, so no claimed chunk is ever dropped
+      s_base = (stop_at != nullptr && ld_cg_u32(stop_at) >= stop_target)
+                   ? 0xFFFFFFFFu
+                   : begin + atomicAdd(cursor, chunk);
       s_next = 0;
     }
     __syncthreads();
@@ -452,24 +562,34 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
 // its own result; only the probing order changes.
 constexpr uint32_t kBinBits = 6;
 constexpr uint32_t kBins = 1u << kBinBits;
+static_assert(kBins == 64, "the region scan gives each lane two regions");
 
 struct BinCounters {
   uint32_t count[kBins];
   uint32_t cursor[kBins];
 };
 
-// Pass 1: per-op region (stored, one byte) and per-region counts.
+// Pass 1: per-op region (stored, one byte) and per-region counts.  Lanes of
+// a warp that fall in the same region add together (hot keys would otherwise
+// serialise on one shared-memory counter).  The keys are read with normal
+// caching: the probe gathers them again in region order.
 template <class Tr>
 __device__ void phase_bin_count(const TableView& t, const Window<Tr>& w, uint8_t* obin,
                                 BinCounters* bc, uint32_t shift) {
   __shared__ uint32_t hist[kBins];
   for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
-  const uint32_t nt = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt) {
-    const uint32_t b = ((uint32_t)Tr::hash(key_stream(w, i)) & t.mask) >> shift;
-    obin[i] = (uint8_t)b;
-    atomicAdd(&hist[b], 1u);
+  const uint32_t nt = gridDim.x * blockDim.x, lane = threadIdx.x & 31u;
+  // warp-uniform loop: every lane runs every round
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < w.n; i0 += nt) {
+    const uint32_t i = i0 + lane;
+    uint32_t b = kBins;
+    if (i < w.n) {
+      b = ((uint32_t)Tr::hash(key_of(w, i)) & t.mask) >> shift;
+      obin[i] = (uint8_t)b;
+    }
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    if (b < kBins && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&hist[b], __popc(peers));
   }
   __syncthreads();
   for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x)
@@ -485,12 +605,15 @@ __device__ void phase_bin_scatter(const Window<Tr>& w, const uint8_t* obin, uint
   __shared__ uint32_t hist[kBins], base[kBins];
   for (uint32_t b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
-  const uint32_t nt = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt)
-    atomicAdd(&hist[obin[i] & (kBins - 1)], 1u);
+  const uint32_t nt = gridDim.x * blockDim.x, lane = threadIdx.x & 31u;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < w.n; i0 += nt) {
+    const uint32_t i = i0 + lane;
+    const uint32_t b = i < w.n ? (obin[i] & (kBins - 1)) : kBins;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    if (b < kBins && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&hist[b], __popc(peers));
+  }
   __syncthreads();
   if (threadIdx.x < 32) {  // region starts: exclusive scan of the 64 counts
-    const uint32_t lane = threadIdx.x;
     const uint32_t c0 = ld_cg_u32(&bc->count[2 * lane]), c1 = ld_cg_u32(&bc->count[2 * lane + 1]);
     uint32_t x = c0 + c1;
 #pragma unroll
@@ -504,9 +627,15 @@ __device__ void phase_bin_scatter(const Window<Tr>& w, const uint8_t* obin, uint
     base[2 * lane + 1] = start0 + c0 + (h1 ? atomicAdd(&bc->cursor[2 * lane + 1], h1) : 0u);
   }
   __syncthreads();
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += nt) {
-    const uint32_t pos = atomicAdd(&base[obin[i] & (kBins - 1)], 1u);
-    if (pos < w.n) perm[pos] = i;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < w.n; i0 += nt) {
+    const uint32_t i = i0 + lane;
+    const uint32_t b = i < w.n ? (obin[i] & (kBins - 1)) : kBins;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, b);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (b < kBins && lane == leader) pos = atomicAdd(&base[b], __popc(peers));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, leader) + __popc(peers & ((1u << lane) - 1u));
+    if (b < kBins && pos < w.n) perm[pos] = i;
   }
 }
 

@@ -67,6 +67,7 @@ inline void alloc_scratch(lsb::Scratch& sc, uint32_t window, uint32_t* status,
   sc.cnt = (WinCounters*)alloc(2 * sizeof(WinCounters));
   sc.obin = (uint8_t*)alloc(window);
   sc.perm = (uint32_t*)alloc(4ull * window);
+  sc.clist = (uint32_t*)alloc(4ull * clist_cap(window));
   sc.hcap = window / (kHugeMin + 1) + 1;
   sc.rcap = window / kRunUnit + sc.hcap;
   sc.hlist = (uint32_t*)alloc(4ull * sc.hcap);

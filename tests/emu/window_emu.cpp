@@ -6,7 +6,11 @@
 // phases against its buffer; the results are written for comparison with
 // the oracle.
 //
-// usage: window_emu <ops file> <log2 buckets> <pool slabs> <block threads> <out file>
+// usage: window_emu <ops file> <log2 buckets> <pool slabs> <block threads> <out file> [mode]
+// mode muts_first: the probe runs as the fused kernel's split-0 form does:
+// the mutation list, the probe of its tiles, then a pass over the reads.
+// mode muts_first_binned: the same with the reads probed in table-region
+// order (region counts beside the list, the scatter beside the list probe).
 // ops file: u32 n, u32 max_window, n x u8 type, n x u64 key, n x u64 value
 // out file: n x lsb_result (u8 found, 7 pad, u64 value), then u32 status
 #include "simt_host.h"
@@ -16,6 +20,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <memory>
 #include <vector>
 
@@ -23,10 +28,12 @@ using namespace lsb;
 using Tr = MapTraits;
 
 int main(int argc, char** argv) {
-  if (argc != 6) {
-    std::fprintf(stderr, "usage: window_emu <ops> <log2> <pool> <block> <out>\n");
+  if (argc != 6 && argc != 7) {
+    std::fprintf(stderr, "usage: window_emu <ops> <log2> <pool> <block> <out> [mode]\n");
     return 2;
   }
+  const bool binned = argc == 7 && std::strcmp(argv[6], "muts_first_binned") == 0;
+  const bool muts_first = binned || (argc == 7 && std::strcmp(argv[6], "muts_first") == 0);
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
   uint32_t n = 0, window = 0;
@@ -64,6 +71,8 @@ int main(int argc, char** argv) {
   emu::alloc_scratch(sc, window, t.status, keep);
   uint8_t* out = (uint8_t*)alloc(16ull * n);
   std::vector<uint32_t> smem(kSortSmemBytes / 4);
+  BinCounters* bins = (BinCounters*)alloc(sizeof(BinCounters));
+  const uint32_t bin_shift = log2 > kBinBits ? log2 - kBinBits : 0u;
 
   uint32_t epoch = 0;
   for (uint32_t off = 0; off < n; off += window) {
@@ -81,6 +90,7 @@ int main(int argc, char** argv) {
     w.out_kind = kOutResult;
     w.cnt = &sc.cnt[0];
     std::memset(sc.cnt, 0, 2 * sizeof(WinCounters));
+    std::memset(bins, 0, sizeof(BinCounters));
     // probe: the library's grid for prefetch 0, static stride
     const unsigned per_sm = 2048 / block;
     const unsigned grid = std::max(1u, std::min(per_sm * num_sms, (m + block - 1) / block));
@@ -88,8 +98,35 @@ int main(int argc, char** argv) {
       emu::run_block(block, b, grid, [&] {
         const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
         const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-        phase_probe<Tr, true, 1>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, 0, false);
+        if (muts_first) {
+          phase_list_muts<Tr>(sc, w, warp, nwarps);
+          if (binned) phase_bin_count<Tr>(t, w, sc.obin, bins, bin_shift);
+        } else {
+          phase_probe<Tr, true, 1>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, 0, false);
+        }
       });
+    if (muts_first) {
+      for (unsigned b = 0; b < grid; ++b)
+        emu::run_block(block, b, grid, [&] {
+          const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+          const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+          const uint32_t listed = std::min(w.cnt->clist_count, clist_cap(sc.max_window));
+          phase_probe_list<Tr>(t, sc, w, warp, nwarps, false);
+          if (binned)
+            phase_bin_scatter<Tr>(w, sc.obin, sc.perm, bins);
+          else  // reads until every list tile is done, as the fused kernel does
+            phase_probe<Tr, false, 1>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, block, false,
+                                      ProbeSel{0, m, false}, 0, nullptr, &w.cnt->tiles_done,
+                                      (listed + 31) / 32);
+        });
+      for (unsigned b = 0; b < grid; ++b)
+        emu::run_block(block, b, grid, [&] {
+          const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+          const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+          phase_probe<Tr, false, 1>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, block, false,
+                                    ProbeSel{0, m, false}, 0, binned ? sc.perm : nullptr);
+        });
+    }
     emu::sort_window<Tr>(sc, w, num_sms, 256, smem);
     const unsigned rgrid = std::max(1u, std::min(num_sms * 8, (m + 255) / 256));
     for (unsigned b = 0; b < rgrid; ++b)

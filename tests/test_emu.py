@@ -92,9 +92,15 @@ def test_ordering_matches_index_order(bins, tmp_path, case, threads, blocks):
     assert r.returncode == 0 and r.stdout.startswith("OK"), r.stdout + r.stderr
 
 
-def test_whole_batch_in_bounds_and_equal_to_oracle(bins, tmp_path):
+@pytest.mark.parametrize("mode,window", [("tiles", 16_384), ("muts_first", 16_383),
+                                         ("muts_first_binned", 16_384)])
+def test_whole_batch_in_bounds_and_equal_to_oracle(bins, tmp_path, mode, window):
     """Probe, ordering (with a group of ~5k mutations) and resolve of a mixed
-    batch over two windows, under AddressSanitizer."""
+    batch over two windows, under AddressSanitizer.  muts_first probes the way
+    the fused kernel's split-0 form does (mutation list, then the reads);
+    muts_first_binned probes the reads in table-region order.  The
+    muts_first window size puts the second window's types off 16-byte
+    alignment and ends the first with a partial span."""
     n, log2 = 24_000, 6
     rng = np.random.default_rng(11)
     t = rng.choice([0, 1, 2], size=n, p=[0.5, 0.35, 0.15]).astype(np.uint8)
@@ -102,10 +108,11 @@ def test_whole_batch_in_bounds_and_equal_to_oracle(bins, tmp_path):
     k[rng.random(n) < 0.45] = np.uint64(77)
     v = W.splitmix64(13, 0, n)
     path, outp = tmp_path / "ops.bin", tmp_path / "out.bin"
-    _write_window(path, t, k, 16_384, v)
+    _write_window(path, t, k, window, v)
     want = OracleMap(log2).mixed(t, k, v)
     pool = (1 << log2) // 4 + 4096
-    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp)],
+    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp)]
+                       + ([mode] if mode != "tiles" else []),
                        capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout + r.stderr[-4000:]
     raw = np.fromfile(outp, np.uint8)

@@ -75,9 +75,10 @@ def _mixed_case(seed, n, key_space, mix=(0.5, 0.35, 0.15)):
     return types, keys, vals
 
 
-@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("fused,split,region", [(False, 100, 0), (True, 100, 0), (True, 0, 0),
+                                                (True, 40, 0), (True, 0, 1), (True, 100, 1)])
 @pytest.mark.parametrize("window", [0, 4096])
-def test_mixed_conflicts_vs_oracle(cuda, fused, window):
+def test_mixed_conflicts_vs_oracle(cuda, fused, split, region, window):
     """Random get/put/remove order over a small key space (heavy same-key
     conflicts inside and across windows): every result and the final contents
     equal the sequential replay."""
@@ -86,6 +87,7 @@ def test_mixed_conflicts_vs_oracle(cuda, fused, window):
     o = OracleMap(log2)
     want = o.mixed(types, keys, vals)
     m = Map(log2, max_window=window)
+    m.set_tuning(fused_split=split, region_order=region)
     out = results_buf(n)
     run = m.execute_fused if fused else m.execute
     run(dev(types), dev(keys), dev(vals), out)
@@ -98,9 +100,11 @@ def test_mixed_conflicts_vs_oracle(cuda, fused, window):
     assert m.status() == 0
 
 
-@pytest.mark.parametrize("fused,block", [(False, 512), (True, 128), (True, 256), (True, 512),
-                                         (True, 1024)])
-def test_hot_key_big_groups(cuda, fused, block):
+@pytest.mark.parametrize("fused,block,split", [(False, 512, 100), (True, 128, 100),
+                                               (True, 256, 100), (True, 512, 100),
+                                               (True, 1024, 100), (True, 256, 0),
+                                               (True, 1024, 0)])
+def test_hot_key_big_groups(cuda, fused, block, split):
     """One key carries ~40k mutations in one window (the multi-step ordering
     of hot keys) and 50 keys ~800 each (block-wide ordering), interleaved
     with reads of them; every launch shape of the fused kernel."""
@@ -113,7 +117,7 @@ def test_hot_key_big_groups(cuda, fused, block):
     o = OracleMap(8)
     want = o.mixed(types, keys, vals)
     m = Map(8)
-    m.set_tuning(block_threads=block)
+    m.set_tuning(block_threads=block, fused_split=split)
     out = results_buf(n)
     (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
     _sync()
@@ -122,8 +126,9 @@ def test_hot_key_big_groups(cuda, fused, block):
     assert m.status() == 0
 
 
-@pytest.mark.parametrize("fused", [False, True])
-def test_huge_skewed_groups(cuda, fused):
+@pytest.mark.parametrize("fused,split,region", [(False, 100, 0), (True, 100, 0), (True, 0, 0),
+                                                (True, 0, 1)])
+def test_huge_skewed_groups(cuda, fused, split, region):
     """Groups far above the shared-memory sort size in one 2^20-op window:
     one key spread over the whole window, one packed densely into a narrow
     index range with a few strays far away (a very uneven spread of member
@@ -140,6 +145,7 @@ def test_huge_skewed_groups(cuda, fused):
     o = OracleMap(10)
     want = o.mixed(types, keys, vals)
     m = Map(10, max_window=n)
+    m.set_tuning(fused_split=split, region_order=region)
     out = results_buf(n)
     (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
     _sync()
@@ -151,7 +157,8 @@ def test_huge_skewed_groups(cuda, fused):
     assert m.status() == 0
 
 
-def test_type_sorted_batches_plain_equals_fused(cuda):
+@pytest.mark.parametrize("split,region", [(0, 0), (100, 0), (0, 1)])
+def test_type_sorted_batches_plain_equals_fused(cuda, split, region):
     """The 95/5 Zipf workload shape at small size: per-op-type calls (gets then
     puts) and the fused path give identical results, equal to the oracle."""
     seed, log2, items = 21, 12, 1 << 16
@@ -160,6 +167,7 @@ def test_type_sorted_batches_plain_equals_fused(cuda):
     o = OracleMap(log2)
     o.put(pk, pv)
     a, b = Map(log2), Map(log2)
+    b.set_tuning(fused_split=split, region_order=region)
     a.put(dev(pk), dev(pv))
     b.put(dev(pk), dev(pv))
     for bi in range(3):
@@ -290,14 +298,15 @@ def test_empty_and_bad_arguments(cuda):
 @pytest.mark.parametrize("block", [256, 1024])
 @pytest.mark.parametrize("prefetch", [0, 1, 2])
 @pytest.mark.parametrize("chunk", [0, 2048])
-def test_every_tuning_is_exact(cuda, block, prefetch, chunk):
+@pytest.mark.parametrize("split", [0, 100])
+def test_every_tuning_is_exact(cuda, block, prefetch, chunk, split):
     """Launch tuning never changes results (fused and per-phase paths)."""
     n, log2 = 40_000, 6
     types, keys, vals = _mixed_case(71, n, key_space=1500)
     want = OracleMap(log2).mixed(types, keys, vals)
     for fused in (True, False):
         m = Map(log2, max_window=8192)
-        m.set_tuning(block_threads=block, prefetch=prefetch, chunk=chunk)
+        m.set_tuning(block_threads=block, prefetch=prefetch, chunk=chunk, fused_split=split)
         out = results_buf(n)
         (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
         _sync()

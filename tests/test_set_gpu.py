@@ -38,9 +38,9 @@ def test_contains_insert_remove_known_answer(cuda):
     assert s.status() == 0
 
 
-@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("fused,split", [(False, 100), (True, 100), (True, 0)])
 @pytest.mark.parametrize("window", [0, 2048])
-def test_set_mixed_conflicts_vs_oracle(cuda, fused, window):
+def test_set_mixed_conflicts_vs_oracle(cuda, fused, split, window):
     n, log2 = 50_000, 5
     rng = np.random.default_rng(8)
     types = rng.choice([OP_CONTAINS, OP_INSERT, OP_REMOVE], size=n, p=[0.5, 0.4, 0.1])
@@ -50,6 +50,7 @@ def test_set_mixed_conflicts_vs_oracle(cuda, fused, window):
     o = OracleSet(log2)
     want = o.mixed(types, keys)
     s = Set(log2, max_window=window)
+    s.set_tuning(fused_split=split)
     out = _bools(n, cuda)
     (s.execute_fused if fused else s.execute)(dev(types), dev(keys), out)
     cuda.cuda.synchronize()
