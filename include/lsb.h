@@ -88,7 +88,8 @@ typedef struct lsb_tuning {
   uint32_t block_threads; /* threads per block: 128, 256, 512 or 1024 (4..32 warps) */
   uint32_t chunk;         /* ops a block claims per step in the probe phase (its warps
                              share them out), multiple of 32 up to 2^20; 0 = static
-                             grid stride */
+                             grid stride.  With fused_split 0: the claim size of the
+                             reads of the fused path; 0 = one tile per warp */
   uint32_t prefetch;      /* extra lookups a thread keeps in flight: 0, 1 or 2 */
   uint32_t dedup;         /* 1: lanes of a warp carrying the same key share one lookup */
   uint32_t fused_split;   /* fused path: percent of a window's reads probed before the
@@ -251,8 +252,9 @@ int lsb_graph_destroy(lsb_graph* g);
 
 /* Autotuner: times the fused path on a sample batch for every block size
  * (256, 512, 1024 threads = 8, 16, 32 warps), lookahead (0, 1, 2) and probe
- * order (mutations listed and probed first, reads meanwhile and after; or
- * all ops in one pass with claim size static, 1024, 2048 or 4096 ops),
+ * order: mutations listed and probed first, reads meanwhile and after, with
+ * a read claim size of one tile per warp, 2048, 4096, 8192 or 16384 ops; or
+ * all ops in one pass with claim size static, 1024, 2048 or 4096 ops.  It
  * keeps the fastest on the table
  * and in a process-wide cache by table size that tables created later with
  * the same log2_buckets start from.  The sample is applied once per

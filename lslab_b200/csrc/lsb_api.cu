@@ -150,6 +150,10 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     // sort pass, where they fill the SMs that the (latency-bound, few-block)
     // ordering of big groups leaves idle.  Reads do not depend on the groups.
     const uint32_t split = (uint32_t)(((uint64_t)w.n * job.split_q16) >> 16);
+    // ops a block claims at a time for the reads probed beside the mutation
+    // list and the ordering pass: the tuned claim size (split 0 has no other
+    // use for it), else one tile per warp
+    const uint32_t late_chunk = (split == 0 && job.chunk) ? job.chunk : blockDim.x * P;
     if (split == 0) {
       // Mutations listed, then probed from the list; while their (latency-
       // bound) chains run, blocks take reads from the same cursor as the sort
@@ -164,7 +168,7 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
         phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
         perm = sc.perm;
       } else {
-        phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, blockDim.x * P,
+        phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, late_chunk,
                                   job.dedup != 0, ProbeSel{0, w.n, false}, 0, nullptr,
                                   &w.cnt->tiles_done, (listed + 31) / 32);
       }
@@ -191,9 +195,9 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     if (has_big || split < w.n) {
       if (has_big) phase_sort_big<Tr>(sc, w, smem);
       if (has_huge) huge_hist<Tr>(sc, w, warp, nwarps);
-      if (split < w.n)  // small claims so blocks freed by the sort take more
+      if (split < w.n)  // claimed, so blocks freed by the sort take more
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
-                                  blockDim.x * P, job.dedup != 0, ProbeSel{split, w.n, false},
+                                  late_chunk, job.dedup != 0, ProbeSel{split, w.n, false},
                                   split & ~31u, perm);
       if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     }
@@ -998,13 +1002,14 @@ int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::K
   int err = LSB_OK;
   for (uint32_t block : {256u, 512u, 1024u}) {
     for (uint32_t prefetch : {0u, 1u, 2u}) {
-      // split 0 (mutations listed first) has no claim size to tune
-      for (uint32_t chunk : {0xFFFFFFFFu, 0u, 1024u, 2048u, 4096u}) {
+      // split 0: chunk = the reads' claim size; split 100: the probe's
+      for (uint32_t cand = 0; cand < 9; ++cand) {
+        static const uint32_t kChunks[9] = {0u, 2048u, 4096u, 8192u, 16384u, 0u, 1024u, 2048u, 4096u};
         lsb_tuning c = cur;
         c.block_threads = block;
         c.prefetch = prefetch;
-        c.chunk = chunk == 0xFFFFFFFFu ? 0u : chunk;
-        c.fused_split = chunk == 0xFFFFFFFFu ? 0u : 100u;
+        c.chunk = kChunks[cand];
+        c.fused_split = cand < 5 ? 0u : 100u;
         if (tb.set_tuning(c) != LSB_OK) continue;
         if (tb.fused_grid() <= 0) continue;  // shape cannot be co-resident
         err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);  // warm-up
