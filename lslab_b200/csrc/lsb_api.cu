@@ -108,7 +108,9 @@ __device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t 
 
 // All windows of one batch.  `seq` counts the grid barriers this launch has
 // passed (shared with a caller that runs several batches in one launch).
-template <class Tr, int P>
+// kList: compile the list-first probe order (fused_split 0); the serving
+// loop, whose waves always probe in one pass, leaves it out.
+template <class Tr, int P, bool kList = true>
 __device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
                               GridBarrier* bar, uint32_t* smem, uint32_t& seq) {
   const uint32_t nblocks = gridDim.x;
@@ -154,7 +156,7 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     // list and the ordering pass: the tuned claim size (split 0 has no other
     // use for it), else one tile per warp
     const uint32_t late_chunk = (split == 0 && job.chunk) ? job.chunk : blockDim.x * P;
-    if (split == 0) {
+    if (kList && split == 0) {
       // Mutations listed, then probed from the list; while their (latency-
       // bound) chains run, blocks take reads from the same cursor as the sort
       // pass, until every list tile is done.  Region binning of the reads
@@ -467,7 +469,7 @@ __global__ void __launch_bounds__(1024, 1)
       fj.base.vals = j.d_vals;
       fj.base.out = j.a_out + pos;  // results go straight to the host-mapped arena
       fj.base.n = nops;
-      fused_windows<MapTraits, P>(t, sc, fj, bar, smem, seq);
+      fused_windows<MapTraits, P, false>(t, sc, fj, bar, smem, seq);
     }
     const uint64_t next = first + nreq;
     ++a;

@@ -138,30 +138,6 @@ __device__ __forceinline__ uint32_t ld_ca_u32(const void* p) {
   return r;
 }
 
-// Window scratch (group table, member lists) read in the resolve phase:
-// L1-cached without an L2 policy.  Safe for the same reason as the probe's
-// loads: the scratch is written only in earlier phases, behind a grid
-// barrier or in an earlier launch.  Hot groups' lists then hit L1.
-__device__ __forceinline__ uint32_t ld_l1_u32(const void* p) {
-  uint32_t r;
-  asm volatile("ld.global.ca.u32 %0, [%1];" : "=r"(r) : "l"(p));
-  return r;
-}
-
-__device__ __forceinline__ uint64_t ld_l1_u64(const void* p) {
-  uint64_t r;
-  asm volatile("ld.global.ca.u64 %0, [%1];" : "=l"(r) : "l"(p));
-  return r;
-}
-
-__device__ __forceinline__ uint4 ld_l1_v4(const void* p) {
-  uint4 r;
-  asm volatile("ld.global.ca.v4.u32 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
-               : "l"(p));
-  return r;
-}
-
 // Streaming (read-once / write-once) batch data: evict-first in L1 and L2.
 __device__ __forceinline__ uint64_t ld_cs_u64(const void* p) {
   uint64_t r;

@@ -1134,8 +1134,8 @@ __device__ __forceinline__ void post_state(const Window<Tr>& w, uint32_t p, bool
 // whether i is the group's last mutation.
 __device__ __forceinline__ uint32_t inline_pred(const Scratch& sc, uint32_t gslot, uint32_t c,
                                                 uint32_t i, uint32_t n, bool* last) {
-  const uint4 a = ld_l1_v4(&sc.ginl[(size_t)gslot * kInline]);
-  const uint4 b = ld_l1_v4(&sc.ginl[(size_t)gslot * kInline + 4]);
+  const uint4 a = ld_cg_v4(&sc.ginl[(size_t)gslot * kInline]);
+  const uint4 b = ld_cg_v4(&sc.ginl[(size_t)gslot * kInline + 4]);
   const uint32_t m[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
   uint32_t best = 0xFFFFFFFFu;
   bool later = false;
@@ -1187,94 +1187,52 @@ __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
   }
 }
 
-// Reads after the window's first mutation whose key has a group take the
-// post-state of their predecessor mutation (the last member before them);
-// the others keep the probe's result.  Each thread resolves two reads at a
-// time with their load chains interleaved (the chains are dependent loads:
-// group table, owner key, then a binary search of big groups' sorted lists).
 template <class Tr>
 __device__ void phase_resolve_reads(const Scratch& sc, const Window<Tr>& w, uint32_t tid,
                                     uint32_t nthreads) {
-  using Key = typename Tr::Key;
-  constexpr int R = 2;
   const uint32_t first = ~ld_cg_u32(&w.cnt->inv_first_mut);
   if (first >= w.n) return;
-  for (uint32_t i0 = first + 1 + tid; i0 < w.n; i0 += R * nthreads) {
-    uint32_t idx[R], slot[R], c[R], lo[R], hi[R], off[R], pred[R];
-    Key key[R];
-    uint8_t type[R];
-    bool open[R], hit[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      idx[r] = i0 + r * nthreads;
-      type[r] = idx[r] < w.n ? op_type(w, idx[r]) : kOpWrite;
-      open[r] = type[r] == kOpRead;
-      hit[r] = false;
-      key[r] = open[r] ? key_of(w, idx[r]) : (Key)0;
-      slot[r] = gslot_of(Tr::hash(key[r]), sc.gmask);
-      c[r] = 0;
-      pred[r] = 0xFFFFFFFFu;
-      lo[r] = hi[r] = off[r] = 0;
-    }
-    // group table: linear probing until an empty (stale-epoch) slot or the key
-    for (uint32_t probe = 0; probe <= sc.gmask && (open[0] || open[1]); ++probe) {
-      uint64_t v[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[r] = open[r] ? ld_l1_u64(&sc.gtab[slot[r]]) : 0ull;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (!open[r]) continue;
-        if (g_epoch(v[r]) != w.epoch) {
-          open[r] = false;
-        } else if (key_of(w, g_owner(v[r]) - 1) == key[r]) {
-          open[r] = false;
-          hit[r] = true;
-          c[r] = g_count(v[r]);
-        } else {
-          slot[r] = (slot[r] + 1) & sc.gmask;
-        }
+  for (uint32_t i = first + 1 + tid; i < w.n; i += nthreads) {
+    const uint8_t type = op_type(w, i);
+    if (type != kOpRead) continue;
+    const typename Tr::Key key = key_of(w, i);
+    const uint64_t h = Tr::hash(key);
+    uint32_t slot = gslot_of(h, sc.gmask);
+    uint64_t v = 0;
+    bool hit = false;
+    for (uint32_t probe = 0; probe <= sc.gmask; ++probe) {
+      v = ld_relaxed_u64(&sc.gtab[slot]);
+      if (g_epoch(v) != w.epoch) break;
+      if (key_of(w, g_owner(v) - 1) == key) {
+        hit = true;
+        break;
       }
+      slot = (slot + 1) & sc.gmask;
     }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (!hit[r]) continue;
-      if (c[r] <= kInline) {
-        bool last;
-        pred[r] = inline_pred(sc, slot[r], c[r], idx[r], w.n, &last);
-      } else {
-        off[r] = ld_l1_u32(&sc.goff[slot[r]]);
-        if (off[r] > sc.max_window || c[r] > sc.max_window - off[r]) {
-          hit[r] = false;  // never written: keep the probe's result
-          continue;
-        }
-        hi[r] = c[r];  // binary search: count of members < idx
-      }
-    }
-    while (lo[0] < hi[0] || lo[1] < hi[1]) {
-      uint32_t x[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-        x[r] = lo[r] < hi[r] ? ld_l1_u32(&sc.seg[off[r] + ((lo[r] + hi[r]) >> 1)]) : 0u;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (lo[r] >= hi[r]) continue;
-        const uint32_t mid = (lo[r] + hi[r]) >> 1;
-        if (x[r] < idx[r])
-          lo[r] = mid + 1;
+    if (!hit) continue;
+    const uint32_t c = g_count(v);
+    uint32_t pred_op = 0xFFFFFFFFu;
+    if (c <= kInline) {
+      bool last;
+      pred_op = inline_pred(sc, slot, c, i, w.n, &last);
+    } else {
+      const uint32_t off = ld_cg_u32(&sc.goff[slot]);
+      if (off > sc.max_window || c > sc.max_window - off) continue;
+      uint32_t lo = 0, hi = c;  // count of members < i
+      while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ld_cg_u32(&sc.seg[off + mid]) < i)
+          lo = mid + 1;
         else
-          hi[r] = mid;
+          hi = mid;
       }
+      if (lo > 0) pred_op = ld_cg_u32(&sc.seg[off + lo - 1]);
     }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      if (!hit[r]) continue;
-      if (c[r] > kInline && lo[r] > 0) pred[r] = ld_l1_u32(&sc.seg[off[r] + lo[r] - 1]);
-      if (pred[r] < w.n) {
-        bool present;
-        uint64_t value;
-        post_state(w, pred[r], &present, &value);
-        write_result(w, idx[r], type[r], present, value);
-      }
+    if (pred_op < w.n) {
+      bool present;
+      uint64_t value;
+      post_state(w, pred_op, &present, &value);
+      write_result(w, i, type, present, value);
     }
   }
 }
