@@ -93,9 +93,10 @@ typedef struct lsb_tuning {
   uint32_t prefetch;      /* extra lookups a thread keeps in flight: 0, 1 or 2 */
   uint32_t dedup;         /* 1: lanes of a warp carrying the same key share one lookup */
   uint32_t fused_split;   /* fused path: percent of a window's reads probed before the
-                             same-key ordering pass (the rest run during it), 0..100;
-                             0 = the mutations are listed and probed first while blocks
-                             take reads, the remaining reads run during the ordering */
+                             same-key ordering pass (the rest run during it), 0..100,
+                             default 100; 0 = the mutations are listed and probed first
+                             while blocks take reads, the remaining reads run during the
+                             ordering (faster on batches with interleaved op types) */
   uint32_t region_order;  /* fused path: 1 = probe a window in table-region order */
 } lsb_tuning;
 

@@ -578,7 +578,7 @@ struct Table {
   uint32_t chunk = 1;  // per-SM pool refill size
   int num_sms = 0;
   Tuning tune;
-  uint32_t split_q16 = 0;  // mutations listed and probed first, reads fill in (fused_split 0)
+  uint32_t split_q16 = 65536;  // every op in one probe pass (fused_split 100)
   uint64_t* trace = nullptr;   // device phase-trace buffer when tracing is on
   BinCounters* bins = nullptr; // inside the counter block (see kCounterBytes)
   uint32_t* fused_epoch = nullptr;  // device counter of fused windows (see k_fused)
