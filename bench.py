@@ -748,6 +748,7 @@ def run_serving(args, world, rank, local):
     seed = rank_seed(args.seed, rank)
     pool_slabs = 24_000_000_000 // 480
     m = L.Map(25, pool_slabs)
+    apply_tuning(args, m)  # the loop's launch shape (block threads, lookahead)
     srv = L.Server(m, max_wave_ops=args.wave_ops, ring_requests=16384, arena_ops=1 << 22)
     off, n, t, k, v = W.serving_pool(seed, 4096)
     mean_n = float(n.mean())
