@@ -89,6 +89,9 @@ def parse():
     ap.add_argument("--single", action="store_true",
                     help="fused timing only (one table, no plain/e2e/cpu legs): the small "
                          "case for profiler captures")
+    ap.add_argument("--plain", action="store_true",
+                    help="with --single: time the per-op-type calls (a get call and a put "
+                         "call per batch) instead of the fused kernel")
     return ap.parse_args()
 
 
@@ -267,14 +270,23 @@ def run_ours(args, world, rank, local):
     n_get = [int(np.sum(b.types == 0)) for b in batches]
     if args.single:
         ops = n * args.steps
+        old_p = torch.empty(n, dtype=torch.int64, device="cuda")
+
+        def step(b):
+            if args.plain:  # gets then puts: the batch's own order
+                g = n_get[b]
+                fused.get(d_keys[b][:g], out_f[b])
+                fused.put(d_keys[b][g:], d_vals[b][g:], old_p[:n - g])
+            else:
+                fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+
         for b in range(args.warmup):
-            fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+            step(b)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
         for s in range(args.steps):
-            b = args.warmup + s
-            fused.execute_fused(d_types[b], d_keys[b], d_vals[b], out_f[b])
+            step(args.warmup + s)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
