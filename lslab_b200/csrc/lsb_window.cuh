@@ -419,8 +419,9 @@ __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc
   probe_ops<Tr, kGroup, P>(t, sc, w, lane, dedup, idx, type, active, key);
 }
 
-// Phase A for the mutations of a window alone (its reads are probed in a
-// later pass), in two grid steps with a grid barrier between them.
+// Phase A for the mutations of a window (its reads are probed by blocks
+// with no list tile left and in the ordering pass), in two grid steps with a
+// grid barrier between them.
 // Step 1 (phase_list_muts): a warp takes 512-op spans; each lane reads the
 // types of 16 consecutive ops with one 16-byte load, and the span's mutations
 // are appended in op-index order to a list, padded to whole 32-entry tiles
@@ -438,6 +439,7 @@ template <class Tr>
 __device__ void phase_list_muts(const Scratch& sc, const Window<Tr>& w, uint32_t warp_id,
                                 uint32_t num_warps) {
   constexpr uint32_t kPer = kListSpan / 32;
+  static_assert(kPer == 16, "one 16-byte type load and a 16-bit mask per lane");
   if (w.types == nullptr && w.uniform == kOpRead) return;
   const uint32_t lane = lane_id();
   const uint32_t cap = clist_cap(sc.max_window);
