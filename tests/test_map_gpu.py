@@ -195,6 +195,49 @@ def test_type_sorted_batches_plain_equals_fused(cuda, split, region):
     assert np.array_equal(kb, ko) and np.array_equal(vb, vo)
 
 
+@pytest.mark.parametrize("block,split", [(1024, 100), (512, 100), (512, 0)])
+def test_queue_of_batches_in_one_launch(cuda, block, split):
+    """The headline form: several type-sorted 95/5 batches back to back in one
+    buffer, drained by one fused launch (one window per batch), give the
+    results and contents of the per-op-type calls batch by batch and of the
+    sequential replay."""
+    seed, log2, items, nb, bn = 33, 12, 1 << 16, 6, 1 << 14
+    pk = W.prefill_keys(seed, items)
+    pv = W.prefill_values(pk)
+    o = OracleMap(log2)
+    o.put(pk, pv)
+    q, p = Map(log2, max_window=bn), Map(log2)
+    q.set_tuning(block_threads=block, fused_split=split)
+    q.put(dev(pk), dev(pv))
+    p.put(dev(pk), dev(pv))
+    batches = [W.map_zipf_batch(seed, b, bn, items, 0.99, (0.95, 0.05)) for b in range(nb)]
+    types = np.concatenate([b.types for b in batches])
+    keys = np.concatenate([b.keys for b in batches])
+    vals = np.concatenate([b.vals for b in batches])
+    want = o.mixed(types, keys, vals)
+    out = results_buf(len(keys))
+    q.execute_fused(dev(types), dev(keys), dev(vals), out)
+    _sync()
+    got = results(out)
+    assert same_results(got, want), first_mismatch(got, want)
+    for bi, bt in enumerate(batches):
+        ng = int(np.sum(bt.types == OP_GET))
+        outg = results_buf(ng)
+        old = cuda.zeros(bn - ng, dtype=cuda.int64, device="cuda")
+        p.get(dev(bt.keys[:ng]), outg)
+        p.put(dev(bt.keys[ng:]), dev(bt.vals[ng:]), old)
+        _sync()
+        w = want[bi * bn:(bi + 1) * bn]
+        assert same_results(results(outg), w[:ng]), first_mismatch(results(outg), w[:ng])
+        assert np.array_equal(host(old, np.uint64), w["value"][ng:])
+    kq, vq = q.dump()
+    kp, vp = p.dump()
+    ko, vo = o.dump()
+    assert np.array_equal(kq, ko) and np.array_equal(vq, vo)
+    assert np.array_equal(kp, ko) and np.array_equal(vp, vo)
+    assert q.status() == 0 and p.status() == 0
+
+
 def test_remove_then_reinsert(cuda):
     """Remove half, re-put some (same-key revival), get all; also the
     AoS put form (map.h:189-192)."""
