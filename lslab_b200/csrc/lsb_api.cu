@@ -106,13 +106,21 @@ __device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t 
   tr[at++] = (ns << 8) | ((uint64_t)(wi & 0x3F) << 2) | ph;
 }
 
+// Work for warp 0 of block 0 while the rest of the grid resolves the last
+// window (the serving loop admits its next wave there).
+struct NoHook {
+  static constexpr bool kActive = false;
+  __device__ void operator()() const {}
+};
+
 // All windows of one batch.  `seq` counts the grid barriers this launch has
 // passed (shared with a caller that runs several batches in one launch).
 // kList: compile the list-first probe order (fused_split 0); the serving
 // loop, whose waves always probe in one pass, leaves it out.
-template <class Tr, int P, bool kList = true>
+template <class Tr, int P, bool kList = true, class Hook = NoHook>
 __device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
-                              GridBarrier* bar, uint32_t* smem, uint32_t& seq) {
+                              GridBarrier* bar, uint32_t* smem, uint32_t& seq,
+                              const Hook& hook = Hook{}) {
   const uint32_t nblocks = gridDim.x;
   // spread indices: small windows use many SMs; tid 0 is still thread 0 of block 0
   const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
@@ -212,24 +220,29 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
       if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     }
     trace_mark(job.trace, tat, wi, 2);
-    if (has_mut) {
+    // with a hook, warp 0 (threads 0..31 of block 0) runs it during the last
+    // window's resolve and takes no resolve work
+    const uint32_t r0 = Hook::kActive ? 32u : 0u;
+    if (Hook::kActive && wi + 1 == nwin && tid < 32) hook();
+    if (has_mut && tid >= r0) {
       // Mutations and the reads after the first mutation resolve
       // independently.  A small window (every thread holds at most one item
       // of each kind) runs them side by side on two shares of the grid, so
       // it pays one latency chain instead of two; a large one runs them one
       // after the other on the whole grid (mutations cost more per item).
+      const uint32_t rt = tid - r0, rn = nt - r0;
       const uint64_t m = ld_cg_u32(&w.cnt->mut_count);
       const uint32_t first = ~ld_cg_u32(&w.cnt->inv_first_mut);
       const uint64_t r = first < w.n ? w.n - first - 1 : 0;
       const uint32_t ms = (uint32_t)((m + 31) / 32 * 32);
-      if (m + r + 32 <= nt) {
-        if (tid < ms)
-          phase_resolve_mutations<Tr>(t, sc, w, tid, ms);
+      if (m + r + 32 <= rn) {
+        if (rt < ms)
+          phase_resolve_mutations<Tr>(t, sc, w, rt, ms);
         else
-          phase_resolve_reads<Tr>(sc, w, tid - ms, nt - ms);
+          phase_resolve_reads<Tr>(sc, w, rt - ms, rn - ms);
       } else {
-        phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
-        phase_resolve_reads<Tr>(sc, w, tid, nt);
+        phase_resolve_mutations<Tr>(t, sc, w, rt, rn);
+        phase_resolve_reads<Tr>(sc, w, rt, rn);
       }
     }
     // Before the next window: its probes must see this window's writes, and
@@ -417,6 +430,18 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
   }
 }
 
+// The serving loop's hook: admit the next wave (non-blocking) while the grid
+// resolves the current one.
+struct AdmitNext {
+  static constexpr bool kActive = true;
+  const TableView* t;
+  const ServeJob* j;
+  WaveDesc* out;
+  uint64_t head;
+  uint64_t in_flight_puts;
+  __device__ void operator()() const { serve_admit(*t, *j, out, head, false, in_flight_puts); }
+};
+
 template <int P>
 __global__ void __launch_bounds__(1024, 1)
     k_serve(TableView t, Scratch sc, ServeJob j, GridBarrier* bar) {
@@ -469,11 +494,14 @@ __global__ void __launch_bounds__(1024, 1)
       fj.base.vals = j.d_vals;
       fj.base.out = j.a_out + pos;  // results go straight to the host-mapped arena
       fj.base.n = nops;
-      fused_windows<MapTraits, P, false>(t, sc, fj, bar, smem, seq);
+      // the next wave is admitted by warp 0 while the others resolve this one
+      fused_windows<MapTraits, P, false>(
+          t, sc, fj, bar, smem, seq,
+          AdmitNext{&t, &j, &j.wave[(a + 1) & 1], first + nreq, wave_puts});
     }
     const uint64_t next = first + nreq;
     ++a;
-    if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, false, wave_puts);
+    if (tid < 32 && nops == 0) serve_admit(t, j, &j.wave[a & 1], next, false, wave_puts);
     if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
     if (tid == 0) {
       win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
