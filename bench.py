@@ -492,6 +492,7 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, batches)
+        line["cpu_umap"] = cpu_umap(args, batches)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -526,6 +527,38 @@ def cpu_baseline(args, batches):
             "sample": f"{nb} batches of {len(batches[0].keys)} ops replayed {reps}x "
                       f"({ops} ops) on the full-size table (2^{args.buckets_log2} buckets, "
                       f"2^{args.prefill_log2} prefill): {dt:.2f} s wall on {threads} threads"}
+
+
+def cpu_umap(args, batches):
+    """std::unordered_map<uint64_t, uint64_t> host replay of a bounded sample of
+    the same workload (oracle/umap_replay.cpp): the prefill keys in per-core
+    shard maps (filled in parallel, untimed), then the sample batches replayed
+    in op-index order by one thread, and by one thread per shard."""
+    from oracle import UmapReplay
+    shards = max(1, min(32, os.cpu_count() or 1))
+    pk, pv = prefill_arrays(args, 0)
+    u = UmapReplay(pk, pv, shards=shards)
+    nb = min(args.cpu_batches, len(batches))
+    out = {}
+    for threads in (1, shards):
+        ops, dt, reps = 0, 0.0, 0
+        while dt < args.cpu_seconds / 2:
+            for b in batches[:nb]:
+                t, _ = u.replay(b.types, b.keys, b.vals, threads=threads, want_results=False)
+                dt += t
+                ops += len(b.keys)
+            reps += 1
+        out[threads] = (ops / dt / 1e6, ops, dt, reps)
+    u.close()
+    v1, ops1, dt1, reps1 = out[1]
+    vs, opss, dts, repss = out[shards]
+    return {"value": round(v1, 2), "unit": "Mops/s", "cores": 1,
+            "kind": "std::unordered_map replay",
+            "sample": f"{nb} batches of {len(batches[0].keys)} ops replayed {reps1}x ({ops1} ops, "
+                      f"{dt1:.2f} s, steady_clock) after a 2^{args.prefill_log2}-key prefill",
+            "sharded_value": round(vs, 2), "sharded_cores": shards,
+            "sharded_sample": f"the same batches {repss}x ({opss} ops, {dts:.2f} s), one thread "
+                              f"per hash shard, each in op-index order"}
 
 
 # ------------------------------------------------------------ reference arm

@@ -3,6 +3,8 @@
 Python bindings of the checkers:
   * OracleMap / OracleSet — the plain-C restatement of the reference's slab
     list (lsb_oracle.c), run on the host in op-index order;
+  * UmapReplay — the op stream replayed on std::unordered_map (umap_replay.cpp),
+    the host replay reported as a CPU baseline;
   * RefMap / RefSet — the reference's OWN kernels (lslab::map / lslab::set,
     built for sm_100a from the reference headers into _ref/liblslab_ref.so)
     behind a small C-ABI harness; these need a GPU.
@@ -20,6 +22,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liblsb_oracle.so"
+UMAP_LIB = HERE / "libumap_replay.so"
 REF_LIB = HERE / "_ref" / "liblslab_ref.so"
 REF_INCLUDE = Path("/root/reference/include")
 
@@ -204,6 +207,65 @@ class OracleSet:
 
 
 # ------------------------------------------------------------ reference
+_u = None
+
+
+def _ulib():
+    global _u
+    if _u is None:
+        if not UMAP_LIB.exists():
+            build(ref=False)
+        L = C.CDLL(str(UMAP_LIB))
+        P, U32, U64 = C.c_void_p, C.c_uint32, C.c_uint64
+        L.umap_create.restype, L.umap_create.argtypes = P, [U32, P, P, U64]
+        L.umap_replay.restype, L.umap_replay.argtypes = C.c_double, [P, P, P, P, U64, U32, P]
+        L.umap_size.restype, L.umap_size.argtypes = U64, [P]
+        L.umap_destroy.restype, L.umap_destroy.argtypes = None, [P]
+        _u = L
+    return _u
+
+
+class UmapReplay:
+    """std::unordered_map<uint64_t, uint64_t> split into `shards` maps by key
+    hash, prefilled with (keys, vals).  replay() runs a batch in op-index
+    order with one thread, or one thread per shard, and returns (seconds,
+    results) with results in the oracle's result layout."""
+
+    def __init__(self, keys, vals, shards: int = 1):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        vals = np.ascontiguousarray(vals, np.uint64)
+        self.shards = int(shards)
+        self._h = _ulib().umap_create(self.shards, keys.ctypes.data, vals.ctypes.data, len(keys))
+        if not self._h:
+            raise MemoryError("umap_create failed")
+
+    def replay(self, types, keys, vals, threads: int = 1, want_results: bool = True):
+        types = np.ascontiguousarray(types, np.uint8)
+        keys = np.ascontiguousarray(keys, np.uint64)
+        vals = np.ascontiguousarray(vals, np.uint64)
+        out = np.zeros(len(keys), RESULT_DTYPE) if want_results else None
+        dt = _ulib().umap_replay(self._h, types.ctypes.data, keys.ctypes.data, vals.ctypes.data,
+                                 len(keys), int(threads),
+                                 out.ctypes.data if out is not None else None)
+        if dt < 0:
+            raise ValueError("threads must be 1 or the shard count")
+        return dt, out
+
+    def size(self) -> int:
+        return int(_ulib().umap_size(self._h))
+
+    def close(self):
+        if self._h:
+            _ulib().umap_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def ref_available() -> bool:
     return REF_LIB.exists()
 

@@ -8,7 +8,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from oracle import OracleMap, OracleSet, ref_map_pool_bound
+from oracle import OracleMap, OracleSet, UmapReplay, ref_map_pool_bound
 from lslab_b200 import workload as W
 
 GOLD = Path(__file__).resolve().parent / "golden"
@@ -127,6 +127,28 @@ def test_oracle_equals_dict_replay(seed):
     k, vv = o.dump()
     assert len(k) == len(d)
     assert all(d[int(a)] == int(b) for a, b in zip(k, vv))
+
+
+@pytest.mark.parametrize("shards,threads", [(1, 1), (4, 1), (4, 4)])
+def test_unordered_map_replay_equals_oracle(shards, threads):
+    """The std::unordered_map host replay (the reported CPU baseline) gives the
+    oracle's results on a prefilled map under a mixed Zipf batch with
+    removes and re-puts, single-threaded and one thread per shard."""
+    seed, log2 = 5, 8
+    pk = W.prefill_keys(seed, 1 << 12)
+    pv = W.prefill_values(pk)
+    o = OracleMap(log2)
+    o.put(pk, pv)
+    u = UmapReplay(pk, pv, shards=shards)
+    for b in range(3):
+        bt = W.map_zipf_batch(seed, b, 1 << 14, 1 << 13, 0.99, (0.6, 0.3, 0.1), type_sort=False)
+        want = o.mixed(bt.types, bt.keys, bt.vals)
+        dt, got = u.replay(bt.types, bt.keys, bt.vals, threads=threads)
+        assert dt >= 0
+        assert np.array_equal(got["found"], want["found"])
+        assert np.array_equal(got["value"], want["value"])
+    assert u.size() == len(o.dump()[0])
+    u.close()
 
 
 def test_oracle_multithreaded_equals_single():
