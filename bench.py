@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="zipf9505",
-                    choices=["zipf9505", "batches", "serving", "sets", "locks"],
+                    choices=["zipf9505", "batches", "serving", "sets", "locks", "plain-small"],
                     help="zipf9505: the headline line; batches: 4096 uneven mixed batches in "
                          "one graph-captured fused launch vs per-op-type calls; serving: the "
                          "request loop under open-loop Poisson load")
@@ -982,6 +982,71 @@ def run_locks(args, world, rank, local):
                           "rows": rows}), flush=True)
 
 
+def run_plain_small(args, world, rank, local):
+    """Plain method, small size: map with 2^16 buckets, 2^20 distinct
+    splitmix64 keys inserted (value = key ^ 0x9E3779B97F4A7C15), then 2^20
+    gets (half present keys, half keys of a disjoint stream) in batches of
+    2^16, one get call per batch; this library's lsb_map_get against lslab's
+    own map::get (built for sm_100a) on the same keys, results compared."""
+    import torch
+    import lslab_b200 as L
+    import oracle
+    from oracle import RefMap, ref_map_pool_bound
+    from lslab_b200 import workload as W
+    from lslab_b200.shard import rank_seed
+
+    if rank != 0:
+        return
+    seed = rank_seed(args.seed, rank)
+    nk, bn = 1 << 20, 1 << 16
+    pk = W.prefill_keys(seed, nk)
+    pv = W.prefill_values(pk)
+    rng = np.random.default_rng(seed)
+    present = pk[rng.integers(0, nk, size=nk // 2)]
+    absent = W.absent_keys(seed, nk // 2 + 64, pk)[: nk // 2]
+    q = np.concatenate([present, absent])
+    q = q[rng.permutation(len(q))]
+    dq = dev_u64(torch, q)
+    reps = max(1, args.steps)
+
+    def timed(get, out):
+        for b in range(0, nk, bn):  # warm-up pass
+            get(dq[b:b + bn], out[b:b + bn])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            for b in range(0, nk, bn):
+                get(dq[b:b + bn], out[b:b + bn])
+        e1.record()
+        torch.cuda.synchronize()
+        return nk * reps / (e0.elapsed_time(e1) * 1e-3) / 1e6
+
+    res = {}
+    m = L.Map(16, max(4096, nk // 28 * 2))
+    m.put(dev_u64(torch, pk), dev_u64(torch, pv))
+    out_m = torch.empty((nk, 2), dtype=torch.int64, device="cuda")
+    res["ours_mops"] = round(timed(lambda k, o: m.get(k, o), out_m), 1)
+    status = m.status()
+    if oracle.ref_available():
+        r = RefMap(16, ref_map_pool_bound(16, pk))
+        old = torch.empty(nk, dtype=torch.int64, device="cuda")
+        r.put(dev_u64(torch, pk), dev_u64(torch, pv), old)
+        out_r = torch.empty((nk, 2), dtype=torch.int64, device="cuda")
+        res["lslab_mops"] = round(timed(lambda k, o: r.get(k, o), out_r), 1)
+        a, b = out_m.cpu().numpy(), out_r.cpu().numpy()
+        found_m = (a[:, 0].view(np.uint64) & np.uint64(0xFF)) != 0
+        found_r = (b[:, 0].view(np.uint64) & np.uint64(0xFF)) != 0
+        res["results_identical"] = bool(np.array_equal(found_m, found_r) and np.array_equal(
+            a[:, 1][found_m], b[:, 1][found_r]))
+        res["ours_over_lslab"] = round(res["ours_mops"] / res["lslab_mops"], 2)
+        r.close()
+    hits = int(((out_m[:, 0] & 0xFF) != 0).sum())
+    print(json.dumps({"workload": "plain-small", "description": run_plain_small.__doc__.split(";")[0],
+                      "gets": nk, "batch_ops": bn, "reps": reps, "hit_fraction": hits / nk,
+                      **res, "device_status": status}), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -995,6 +1060,8 @@ def main():
         run_sets(args, world, rank, local)
     elif args.workload == "locks":
         run_locks(args, world, rank, local)
+    elif args.workload == "plain-small":
+        run_plain_small(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
     if world > 1:
