@@ -463,8 +463,12 @@ __global__ void __launch_bounds__(1024, 1)
   // Admission `a` writes descriptor a & 1, which every block finished
   // reading before the barrier of admission a - 1.
   uint32_t a = 0;
+  // Barriers behind a blocking admission wait as long as the admission may
+  // (idle_polls polls of ~2-4 us each; a barrier poll takes >= ~0.1 us).
+  const uint32_t idle_limit =
+      (uint32_t)min(0xFFFFFFFFull, (unsigned long long)kBarrierPolls + 32ull * j.idle_polls);
   if (tid < 32) serve_admit(t, j, &j.wave[0], head, true, 0);
-  if (!grid_barrier(bar, gridDim.x, t.status, seq)) goto out;
+  if (!grid_barrier(bar, gridDim.x, t.status, seq, idle_limit)) goto out;
   for (;;) {
     const WaveDesc* cur = &j.wave[a & 1];
     const uint64_t first = ld_cg_u64(&cur->first), op_off = ld_cg_u64(&cur->op_off);
@@ -516,7 +520,7 @@ __global__ void __launch_bounds__(1024, 1)
       // the queue was empty: wait for requests now that wave k is published
       ++a;
       if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, true, 0);
-      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+      if (!grid_barrier(bar, gridDim.x, t.status, seq, idle_limit)) break;
     }
   }
 out:

@@ -725,16 +725,17 @@ __device__ __forceinline__ void table_apply_known(const TableView& t, typename T
 // a launch completes when the arrival counter reaches (k + 1) * nblocks, so
 // nothing is reset between barriers.  One thread per block arrives with an
 // acquire-release add and polls with acquire loads; the block's other threads are
-// ordered by __syncthreads on both sides.  Each wait polls at most
-// kBarrierPolls times; on timeout it raises kStatusBarrier and returns false
-// so the caller can leave the kernel.
+// ordered by __syncthreads on both sides.  Each wait polls at most `limit`
+// times (kBarrierPolls unless the caller knows a block may legitimately be
+// late for longer); on timeout it raises kStatusBarrier and returns false so
+// the caller can leave the kernel.
 struct GridBarrier {
   uint32_t count;  // arrivals in this launch (zero when a launch starts)
   uint32_t exits;  // blocks that have left the launch (see release_counters)
 };
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, uint32_t* status,
-                                             uint32_t& seq) {
+                                             uint32_t& seq, uint32_t limit = kBarrierPolls) {
   __shared__ int ok;
   __syncthreads();
   ++seq;
@@ -744,7 +745,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, uint32_t nblocks, u
     if (atom_add_acq_rel(&b->count, 1u) + 1 != target) {
       uint32_t it = 0;
       while ((int32_t)(ld_acquire_u32(&b->count) - target) < 0) {
-        if (++it > kBarrierPolls || (*(volatile uint32_t*)status & kStatusBarrier)) {
+        if (++it > limit || (*(volatile uint32_t*)status & kStatusBarrier)) {
           raise_status(status, kStatusBarrier);
           ok = 0;
           break;

@@ -105,6 +105,7 @@ extern "C" int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* ld, uint6
     const uint32_t p = ld->pool_index[i];
     const uint64_t off = ld->pool_off[p];
     uint64_t ticket = 0;
+    const uint64_t tried_from = ns_since(t0);
     for (;;) {
       const int rc = lsb_serve_submit(s, ld->types ? ld->types + off : nullptr, ld->keys + off,
                                       ld->vals ? ld->vals + off : nullptr, ld->pool_n[p], &ticket);
@@ -113,7 +114,14 @@ extern "C" int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* ld, uint6
         error.store(rc);
         break;
       }
-      std::this_thread::yield();  // queue full: the taker frees slots
+      // queue full: the taker frees slots, unless it gave up or the loop
+      // stopped completing requests
+      if (error.load() != LSB_OK) break;
+      if (ns_since(t0) - tried_from > kWaitLimitNs) {
+        error.store(LSB_ERR_TIMEOUT);
+        break;
+      }
+      std::this_thread::yield();
     }
     if (error.load() != LSB_OK) break;
     tickets[i] = ticket;
