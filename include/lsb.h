@@ -186,7 +186,9 @@ int lsb_map_size(lsb_map* m, uint64_t* count, cudaStream_t stream);
  * one static device array shared by all calls: maps of at most 2^20 buckets
  * (larger ones return LSB_ERR_ARG); calls that overlap on the GPU race on the
  * array; the first call on each device resolves the array's address and
- * should come before any stream capture. */
+ * should come before any stream capture (the address is cached for the
+ * process: do not use the library on a device again after cudaDeviceReset).
+ * The current device must be the map's own device (else LSB_ERR_ARG). */
 int lsb_map_size_noalloc(lsb_map* m, uint64_t* count_out, cudaStream_t stream);
 
 /* Copy every live (key, value) pair to HOST arrays, in key order.  *count
@@ -196,22 +198,23 @@ int lsb_map_dump(lsb_map* m, uint64_t* keys_out, uint64_t* vals_out, size_t cap,
                  uint64_t* count, cudaStream_t stream);
 
 /* ---- set<uint32_t> ---------------------------------------------------
- * Replaces lslab::set<K>::set(n_log_2[, Allocator&&]), include/lslab/set.h:267-287. */
+ * Replaces lslab::set<K>::set(n_log_2) (include/lslab/set.h:31-40) and
+ * set(n_log_2, Allocator&&) (include/lslab/set.h:42-51). */
 int lsb_set_create(unsigned log2_buckets, uint64_t pool_slabs, lsb_set** out);
 int lsb_set_create_ex(unsigned log2_buckets, const lsb_options* opt, lsb_set** out);
 int lsb_set_destroy(lsb_set* s);
 
 /* lslab::set::insert<bs>(const K*, bool*, size_t, cudaStream_t),
- * include/lslab/set.h:339-342 -> set_kernels::insert_, set_kernels.h:47-63.
+ * include/lslab/set.h:103-106 -> set_kernels::insert_, set_kernels.h:47-63.
  * Like the reference, out[i] is true for a new AND for an existing key
  * (include/lslab/detail/traverse.h:204-212,226-232). */
 int lsb_set_insert(lsb_set* s, const uint32_t* keys, bool* out, size_t n, cudaStream_t stream);
 
-/* lslab::set::contains<bs>, include/lslab/set.h:328-331 -> set_kernels.h:28-44. */
+/* lslab::set::contains<bs>, include/lslab/set.h:92-95 -> set_kernels.h:28-44. */
 int lsb_set_contains(lsb_set* s, const uint32_t* keys, bool* out, size_t n,
                      cudaStream_t stream);
 
-/* lslab::set::remove<bs>, include/lslab/set.h:350-353 -> set_kernels.h:10-26.
+/* lslab::set::remove<bs>, include/lslab/set.h:114-117 -> set_kernels.h:10-26.
  * out[i] = the key was present. */
 int lsb_set_remove(lsb_set* s, const uint32_t* keys, bool* out, size_t n, cudaStream_t stream);
 
@@ -221,7 +224,7 @@ int lsb_set_execute(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool
 int lsb_set_execute_fused(lsb_set* s, const uint8_t* types, const uint32_t* keys, bool* out,
                           size_t n, cudaStream_t stream);
 
-uint32_t lsb_set_buckets(const lsb_set* s); /* lslab::set::buckets(), set.h:361-363 */
+uint32_t lsb_set_buckets(const lsb_set* s); /* lslab::set::buckets(), set.h:125-127 */
 int lsb_set_get_tuning(const lsb_set* s, lsb_tuning* out);
 int lsb_set_set_tuning(lsb_set* s, const lsb_tuning* t);
 int lsb_set_set_trace(lsb_set* s, int on);

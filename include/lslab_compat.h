@@ -147,25 +147,25 @@ class set<uint32_t> {
     return *this;
   }
 
-  // set.h:328-331
+  // set.h:92-95
   template <int block_size = 256>
   void contains(const uint32_t* keys, bool* output, size_t size, cudaStream_t stream = 0x0) {
     lsb_check(lsb_set_contains(s_, keys, output, size, stream), "lsb_set_contains");
   }
 
-  // set.h:339-342
+  // set.h:103-106
   template <int block_size = 256>
   void insert(const uint32_t* keys, bool* output, size_t size, cudaStream_t stream = 0x0) {
     lsb_check(lsb_set_insert(s_, keys, output, size, stream), "lsb_set_insert");
   }
 
-  // set.h:350-353
+  // set.h:114-117
   template <int block_size = 256>
   void remove(const uint32_t* keys, bool* output, size_t size, cudaStream_t stream = 0x0) {
     lsb_check(lsb_set_remove(s_, keys, output, size, stream), "lsb_set_remove");
   }
 
-  // set.h:361-363
+  // set.h:125-127
   unsigned buckets() const { return lsb_set_buckets(s_); }
 
   lsb_set* handle() const { return s_; }

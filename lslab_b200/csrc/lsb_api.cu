@@ -312,7 +312,8 @@ struct ServeJob {
   uint64_t* d_vals;
   WaveDesc* wave;           // two descriptors, alternating by admission
   uint32_t max_wave_ops;
-  uint32_t idle_polls;
+  uint32_t pad;
+  uint64_t idle_ns;         // a blocking admission waits at most this long (%globaltimer)
   FusedJob<MapTraits> fj;   // engine parameters; base is set per wave
 };
 
@@ -326,15 +327,72 @@ __device__ __forceinline__ void st_release_sys_u64(uint64_t* p, uint64_t v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Warp 0 of block 0: wait (bounded) for requests, then admit the longest
-// FIFO prefix that fits the wave's op limit, whose ops are contiguous in the
-// arena (the host never splits a request across the arena's end) and whose
-// worst-case new slabs (one per put) fit the pool's free slabs.  Lanes read
-// 32 descriptors at a time and admit by warp prefix sums.  A head request
-// that can never fit the pool (slabs are not returned) is refused alone with
-// LSB_ERR_OOM.  `blocking`: wait (bounded) for a request; otherwise an empty
-// queue gives an empty wave.  `in_flight_puts`: puts of a wave still being
-// applied, whose slabs the pool cursor may not show yet.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid barrier behind a blocking admission: it waits until a %globaltimer
+// deadline instead of for a number of polls, so its limit is stated in the
+// same clock as the admission's wait (the caller passes the admission's
+// deadline plus a margin).  Otherwise as grid_barrier.
+__device__ bool grid_barrier_until(GridBarrier* b, uint32_t nblocks, uint32_t* status,
+                                   uint32_t& seq, uint64_t deadline_ns) {
+  __shared__ int ok;
+  __syncthreads();
+  ++seq;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const uint32_t target = seq * nblocks;
+    if (atom_add_acq_rel(&b->count, 1u) + 1 != target) {
+      uint32_t it = 0;
+      while ((int32_t)(ld_acquire_u32(&b->count) - target) < 0) {
+        if ((*(volatile uint32_t*)status & kStatusBarrier) ||
+            ((++it & 255u) == 0 && global_ns() > deadline_ns)) {
+          raise_status(status, kStatusBarrier);
+          ok = 0;
+          break;
+        }
+        if (it > 256) __nanosleep(256);
+      }
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Slabs the pool can still hand out: what the global cursor has left plus
+// what is left in the per-SM ranges (pool_alloc takes those before it
+// reports OOM).  Whole warp; the result is warp-uniform.
+__device__ uint64_t pool_free_slabs(const TableView& t) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t left = 0;
+  for (int k = (int)lane; k < kPoolSlots; k += 32) {
+    const uint64_t v = ld_cg_u64(&t.pool[2 + k]);
+    const uint32_t cur = (uint32_t)v, end = (uint32_t)(v >> 32);
+    left += cur < end ? end - cur : 0u;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) left += __shfl_xor_sync(0xFFFFFFFFu, left, d);
+  const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
+  return left + (limit > cursor ? limit - cursor : 0);
+}
+
+// Warp 0 of block 0: wait (bounded by idle_ns) for requests, then admit the
+// longest FIFO prefix that fits the wave's op limit, whose ops are
+// contiguous in one lap of the arena (the host never splits a request
+// across the arena's end; a request that starts a new lap starts a new
+// wave, so a wave's ops never wrap) and whose worst-case new slabs (one per
+// put) fit the pool's free slabs.  Lanes read 32 descriptors at a time and
+// admit by warp prefix sums.  `blocking`: wait for a request; otherwise an
+// empty queue gives an empty wave.  `in_flight_puts`: puts of a wave still
+// being applied, whose slabs the pool may not show as taken yet; the budget
+// subtracts them in full, so it is a lower bound.  Only an exact budget (no
+// wave in flight) refuses a head request that does not fit: it can never
+// fit (slabs are not returned), so it completes alone with LSB_ERR_OOM;
+// with a wave in flight the admission returns an empty wave instead and the
+// loop retries once that wave is done.
 __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out, uint64_t head,
                             bool blocking, uint64_t in_flight_puts) {
   const uint32_t lane = threadIdx.x & 31;
@@ -343,6 +401,7 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
   uint64_t sub = 0;
   uint32_t stop = 0;
   if (lane == 0) {
+    const uint64_t t0 = blocking ? global_ns() : 0;
     for (uint32_t it = 0;; ++it) {
       sub = ld_acquire_sys_u64(&j.ctl->submitted);
       if (sub > head || !blocking) break;
@@ -350,7 +409,7 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
         stop = 1;
         break;
       }
-      if (it >= j.idle_polls) {
+      if (global_ns() - t0 > j.idle_ns) {
         stop = 2;
         break;
       }
@@ -366,12 +425,8 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
     }
     return;
   }
-  uint64_t budget = 0;
-  if (lane == 0) {
-    const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
-    budget = limit > cursor + in_flight_puts ? limit - cursor - in_flight_puts : 0;
-  }
-  budget = __shfl_sync(0xFFFFFFFFu, budget, 0);
+  const uint64_t free_slabs = pool_free_slabs(t);
+  uint64_t budget = free_slabs > in_flight_puts ? free_slabs - in_flight_puts : 0;
   const uint64_t budget0 = budget;
   const uint64_t end = min(sub, head + j.ring_cap);
   uint32_t nops = 0, nreq = 0;
@@ -394,24 +449,29 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
         cp += yp;
       }
     }
-    // contiguous: this request starts where the previous one ends
+    // contiguous: this request starts where the previous one ends, and not
+    // at the start of a lap (the wave's ops would wrap the arena); the head
+    // request of the wave (base == head, lane 0) is always taken as is
     const uint64_t prev_end = __shfl_up_sync(0xFFFFFFFFu, off + n, 1);
-    const bool contiguous = lane == 0 ? off == next_off : off == prev_end;
+    const bool new_lap = off % j.arena_cap == 0 && !(base == head && lane == 0);
+    const bool contiguous = (lane == 0 ? off == next_off : off == prev_end) && !new_lap;
     const bool fits = valid && contiguous && nops + cn <= j.max_wave_ops && cp <= budget;
     const uint32_t bad = __ballot_sync(0xFFFFFFFFu, !fits);
     const uint32_t take = bad ? (uint32_t)__ffs(bad) - 1 : 32u;
     if (lane < take) q->status = LSB_OK;
     if (take == 0) {
-      if (nreq == 0 && valid && lane == 0 && puts > budget) {
+      // the head request alone does not fit the budget: refuse it only when
+      // the budget is exact (no wave in flight); otherwise admit nothing now
+      const bool refuse = nreq == 0 && in_flight_puts == 0 &&
+                          __shfl_sync(0xFFFFFFFFu, valid && puts > budget, 0);
+      if (refuse && lane == 0) {
         q->status = LSB_ERR_OOM;  // refused alone: no op of it runs
         wd.op_off = off;
         wd.nreq = 1;
         wd.nops = 0;
         *out = wd;
       }
-      if (nreq == 0) {
-        if (__shfl_sync(0xFFFFFFFFu, valid && puts > budget, 0)) return;
-      }
+      if (refuse) return;
       break;
     }
     if (nreq == 0) wd.op_off = __shfl_sync(0xFFFFFFFFu, off, 0);
@@ -463,12 +523,12 @@ __global__ void __launch_bounds__(1024, 1)
   // Admission `a` writes descriptor a & 1, which every block finished
   // reading before the barrier of admission a - 1.
   uint32_t a = 0;
-  // Barriers behind a blocking admission wait as long as the admission may
-  // (idle_polls polls of ~2-4 us each; a barrier poll takes >= ~0.1 us).
-  const uint32_t idle_limit =
-      (uint32_t)min(0xFFFFFFFFull, (unsigned long long)kBarrierPolls + 32ull * j.idle_polls);
+  // Barriers behind a blocking admission wait until the admission's own
+  // deadline (idle_ns from about now) plus a margin, on the same clock.
+  constexpr uint64_t kAdmitMarginNs = 2000000000ull;
   if (tid < 32) serve_admit(t, j, &j.wave[0], head, true, 0);
-  if (!grid_barrier(bar, gridDim.x, t.status, seq, idle_limit)) goto out;
+  if (!grid_barrier_until(bar, gridDim.x, t.status, seq, global_ns() + j.idle_ns + kAdmitMarginNs))
+    goto out;
   for (;;) {
     const WaveDesc* cur = &j.wave[a & 1];
     const uint64_t first = ld_cg_u64(&cur->first), op_off = ld_cg_u64(&cur->op_off);
@@ -478,9 +538,14 @@ __global__ void __launch_bounds__(1024, 1)
       if (tid == 0) *(volatile uint32_t*)&j.ctl->state = stop == 1 ? 2 : 3;
       break;
     }
+    if (nops && (op_off % j.arena_cap) + nops > j.arena_cap) {
+      // cannot happen: admission never lets a wave wrap the arena
+      if (tid == 0) raise_status(t.status, kStatusScratch);
+      break;  // grid-uniform (every block read the same descriptor)
+    }
     if (nops) {
-      // the wave's ops (contiguous in the arena) into HBM; .cv loads because
-      // the host rewrites arena slots between waves
+      // the wave's ops (contiguous in one lap of the arena) into HBM; .cv
+      // loads because the host rewrites arena slots between waves
       const uint64_t pos = op_off % j.arena_cap;
       for (uint32_t i = tid; i < nops; i += nt) {
         // all three loads before any store: they cross PCIe together
@@ -520,7 +585,9 @@ __global__ void __launch_bounds__(1024, 1)
       // the queue was empty: wait for requests now that wave k is published
       ++a;
       if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, true, 0);
-      if (!grid_barrier(bar, gridDim.x, t.status, seq, idle_limit)) break;
+      if (!grid_barrier_until(bar, gridDim.x, t.status, seq,
+                              global_ns() + j.idle_ns + kAdmitMarginNs))
+        break;
     }
   }
 out:
@@ -1132,6 +1199,8 @@ void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buc
   *buckets = m->t.buckets;
 }
 
+int lsb_internal_map_device(const lsb_map* m) { return m->t.device; }
+
 // ------------------------------------------------------------------ serving
 // Host side of the request loop (see k_serve).  One producer may submit while
 // another thread takes results; both advance FIFO cursors.
@@ -1145,7 +1214,8 @@ struct lsb_server {
   uint64_t* a_vals = nullptr;
   lsb_result* a_out = nullptr;
   uint64_t ring_cap = 0, arena_cap = 0;
-  uint32_t max_wave_ops = 0, idle_polls = 0;
+  uint32_t max_wave_ops = 0;
+  uint64_t idle_ns = 0;
   uint8_t* d_types = nullptr;  // HBM working copy of a wave
   uint64_t* d_keys = nullptr;
   uint64_t* d_vals = nullptr;
@@ -1494,9 +1564,7 @@ int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out)
   s->ring_cap = ring;
   s->arena_cap = arena;
   s->max_wave_ops = wave;
-  // idle limit in polls of ~2 us (the admit loop's back-off)
-  s->idle_polls = (uint32_t)std::min<uint64_t>(0xFFFFFFFFull,
-                                                (uint64_t)(o.idle_ms ? o.idle_ms : 10000) * 500);
+  s->idle_ns = (uint64_t)(o.idle_ms ? o.idle_ms : 10000) * 1000000ull;
   s->taken.assign(ring, 0);
   int prev = 0;
   cudaGetDevice(&prev);
@@ -1551,7 +1619,7 @@ int lsb_serve_start(lsb_server* s) {
   j.d_vals = s->d_vals;
   j.wave = s->d_wave;
   j.max_wave_ops = s->max_wave_ops;
-  j.idle_polls = s->idle_polls;
+  j.idle_ns = s->idle_ns;
   if (!j.ctl || !j.ring || !j.a_types || !j.a_keys || !j.a_vals || !j.a_out) {
     cudaSetDevice(prev);
     return LSB_ERR_CUDA;

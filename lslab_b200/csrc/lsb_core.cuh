@@ -304,9 +304,6 @@ struct TableView {
   uint32_t chunk;      // slabs per per-SM refill (smaller for small pools)
 };
 
-constexpr int kPoolSlots = 256;
-constexpr uint32_t kPoolChunkMax = 32;
-
 // ------------------------------------------------------------ slab pool
 // Per-SM bump ranges refilled in chunks from one global cursor.  A range is
 // one u64 {end:32 | cur:32}; atomicAdd on it hands out cur.  Exactly one
@@ -318,7 +315,31 @@ constexpr uint32_t kPoolChunkMax = 32;
 // are never returned, so a slab is always empty when handed out.  Replaces
 // the reference's single global fetch_add with __trap on overflow
 // (include/lslab/detail/device_allocator.h:63-70): here exhaustion returns 0
-// and raises kStatusOOM.
+// and raises kStatusOOM, and only once every slab is handed out: when the
+// global cursor is spent, the slabs still left in other SMs' ranges are taken
+// (pool_alloc_leftover), so a caller that counts free slabs as the cursor's
+// remainder plus the ranges' leftovers (pool_free_slabs) never sees an OOM
+// within that count.
+constexpr int kPoolSlots = 256;
+constexpr uint32_t kPoolChunkMax = 32;
+
+inline __device__ __noinline__ uint32_t pool_alloc_leftover(const TableView& t, uint32_t smid) {
+  for (int k = 0; k < kPoolSlots; ++k) {
+    unsigned long long* range =
+        (unsigned long long*)&t.pool[2 + ((smid + (uint32_t)k) & (kPoolSlots - 1))];
+    unsigned long long v = ld_relaxed_u64((const uint64_t*)range);
+    for (;;) {
+      const uint32_t cur = (uint32_t)v, end = (uint32_t)(v >> 32);
+      if (cur >= end) break;
+      const unsigned long long prev = atomicCAS(range, v, v + 1ull);
+      if (prev == v) return cur;
+      v = prev;
+    }
+  }
+  raise_status(t.status, kStatusOOM);
+  return 0;
+}
+
 __device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
   const uint32_t smid = sm_id();
   unsigned long long* range = (unsigned long long*)&t.pool[2 + (smid & (kPoolSlots - 1))];
@@ -328,10 +349,7 @@ __device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
   const unsigned long long limit = t.pool[1];
   const unsigned long long take = cur == end ? t.chunk : 1ull;  // refill, or a single slab
   const unsigned long long base = atomicAdd((unsigned long long*)&t.pool[0], take);
-  if (base >= limit) {
-    raise_status(t.status, kStatusOOM);
-    return 0;
-  }
+  if (base >= limit) return pool_alloc_leftover(t, smid);
   if (cur == end) {
     const unsigned long long stop = base + take < limit ? base + take : limit;
     atomicExch(range, (stop << 32) | (base + 1));  // base + 1 == stop: spent again
@@ -636,7 +654,26 @@ __device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, u
           st_cg_u64(slab + kMetaBytes + r.found_slot * Tr::kSlotBytes + 8, val);
         if (!r.found_live) {
           __threadfence();
-          atomicOr(tw, 0x80u << sh);
+          // Revive dead -> live by CAS on our own dead tag: where dead slots
+          // are reusable (kReuseDead) another key may have claimed this slot
+          // since the scan, and an unconditional OR would then mark its busy
+          // claim live and lose this insert.  Other bytes of the word may
+          // change meanwhile (retry); if ours no longer reads dead with our
+          // fingerprint, the slot is gone and the insert starts over.
+          uint32_t cur = ld_cg_u32(tw);
+          bool revived = false;
+          while (((cur >> sh) & 0xFFu) == fp) {
+            const uint32_t prev = atomicCAS(tw, cur, cur | (0x80u << sh));
+            if (prev == cur) {
+              revived = true;
+              break;
+            }
+            cur = prev;
+          }
+          if (!revived) {
+            start = bucket;
+            continue;
+          }
         }
       } else if (r.found_live) {
         atomicAnd(tw, ~(0x80u << sh));

@@ -8,3 +8,5 @@
 #include "lsb_core.cuh"
 
 void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buckets);
+// CUDA device the map's memory lives on.
+int lsb_internal_map_device(const lsb_map* m);

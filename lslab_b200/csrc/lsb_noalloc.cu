@@ -22,7 +22,13 @@
 //    race on the array and give wrong counts;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, that device current); make that
-//    first call before starting any stream capture.
+//    first call before starting any stream capture.  The address is cached
+//    for the life of the process: after cudaDeviceReset (or anything else
+//    that tears down the device's primary context) the library must not be
+//    used again on that device;
+//  * the call runs on the current device, which must be the map's own: a map
+//    created on another device is refused with LSB_ERR_ARG (the call neither
+//    switches devices nor reads another GPU's memory).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -114,6 +120,9 @@ extern "C" int lsb_map_size_noalloc(lsb_map* m, uint64_t* count_out, cudaStream_
   TableView view;
   uint32_t buckets = 0;
   lsb_internal_map_view(m, &view, &buckets);
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LSB_ERR_CUDA;
+  if (dev != lsb_internal_map_device(m)) return LSB_ERR_ARG;
   const uint32_t blocks = (buckets + kNoAllocBlock - 1) / kNoAllocBlock;
   if (blocks == 0 || blocks > kNoAllocMaxBlocks) return LSB_ERR_ARG;  // over 2^20 buckets
   unsigned long long* scratch = nullptr;

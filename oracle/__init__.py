@@ -15,6 +15,7 @@ package.  The product (lslab_b200) never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -24,7 +25,17 @@ HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liblsb_oracle.so"
 UMAP_LIB = HERE / "libumap_replay.so"
 REF_LIB = HERE / "_ref" / "liblslab_ref.so"
-REF_INCLUDE = Path("/root/reference/include")
+
+
+def reference_include() -> Path | None:
+    """Include directory of the reference sources (depaulmillz/lslab), used
+    only to build the reference harness: $LSLAB_REFERENCE (the project root)
+    when set, else a checkout named `reference` beside this repository; None
+    when neither holds include/lslab."""
+    env = os.environ.get("LSLAB_REFERENCE")
+    root = Path(env) if env else HERE.parent.parent / "reference"
+    inc = root / "include"
+    return inc if (inc / "lslab").is_dir() else None
 
 
 class OResult(C.Structure):
@@ -42,10 +53,14 @@ def build(ref: bool | None = None) -> None:
     """Compile the oracle (always) and the reference harness (when the
     reference headers are present)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    inc = reference_include()
     if ref is None:
-        ref = REF_INCLUDE.exists()
+        ref = inc is not None
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_INCLUDE={REF_INCLUDE}"],
+        if inc is None:
+            raise RuntimeError("reference sources not found: set LSLAB_REFERENCE to the "
+                               "lslab project root")
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_INCLUDE={inc}"],
                        check=True)
 
 
