@@ -205,3 +205,91 @@ def test_serve_small_arena_wraps_many_laps(cuda):
                               np.concatenate([v[s] for s in seq]))
     assert same_results(res, want), first_mismatch(res, want)
     assert m.status() == 0
+
+
+def test_serve_wave_stops_at_lap_boundary(cuda):
+    """A request that ends exactly at the end of the arena's lap, queued
+    together with one that starts the next lap: they run as separate waves (a
+    wave's ops never wrap the arena), and results equal the replay."""
+    rng = np.random.default_rng(21)
+    sizes = (1000, 1048, 500)  # the second ends at op 2048 = the lap's end
+    reqs = []
+    for n in sizes:
+        t = rng.choice([OP_GET, OP_PUT, OP_REMOVE], size=n, p=[0.4, 0.4, 0.2]).astype(np.uint8)
+        k = W.key_of_rank(21, rng.integers(0, 300, size=n).astype(np.uint64))
+        v = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
+        reqs.append((t, k, v))
+    m = Map(8, max_window=1 << 14)
+    srv = Server(m, max_wave_ops=2048, ring_requests=16, arena_ops=2048)
+    srv.start()
+    got0, st0 = _take_all(srv, reqs[:1], _submit_all(srv, reqs[:1]))
+    first = srv.stop()
+    # queued while the loop is stopped, so one admission sees both
+    tk = _submit_all(srv, reqs[1:])
+    srv.start()
+    got, st = _take_all(srv, reqs[1:], tk)
+    stats = srv.stop()
+    srv.close()
+    assert st0 == [0] and st == [0, 0]
+    assert stats["waves"] - first["waves"] == 2, "the two requests shared a wave across the lap"
+    want = OracleMap(8).mixed(np.concatenate([r[0] for r in reqs]),
+                              np.concatenate([r[1] for r in reqs]),
+                              np.concatenate([r[2] for r in reqs]))
+    g = np.concatenate(got0 + got)
+    assert same_results(g, want), first_mismatch(g, want)
+    assert m.status() == 0
+
+
+def _mix64(k: np.ndarray) -> np.ndarray:
+    """MurmurHash3's 64-bit finaliser, the library's bucket hash."""
+    k = k.astype(np.uint64).copy()
+    with np.errstate(over="ignore"):
+        k ^= k >> np.uint64(33)
+        k *= np.uint64(0xFF51AFD7ED558CCD)
+        k ^= k >> np.uint64(33)
+        k *= np.uint64(0xC4CEB9FE1A85EC53)
+        k ^= k >> np.uint64(33)
+    return k
+
+
+def test_serve_admission_counts_slabs_left_in_sm_ranges(cuda):
+    """A pool large enough for 32-slab per-SM refills, filled until the global
+    cursor is spent while SM ranges still hold unused slabs: a put request
+    that fits those slabs is admitted (not refused) and runs without a device
+    OOM, and results equal the replay."""
+    log2, cap = 10, 40000  # cap / (8 * 148 SMs) >= 32: full-size refills; chains ~40 slabs
+    m = Map(log2, pool_slabs=cap, max_window=1 << 16)
+    mask = np.uint64((1 << log2) - 1)
+    keys = W.prefill_keys(31, 28 * (cap + (1 << log2)))
+    o = OracleMap(log2, 2 * cap)
+    placed = 0
+    for step in (1 << 16, 1 << 14, 1 << 12):
+        while placed + step <= len(keys) and m.pool_usage()[0] < cap:
+            b = keys[placed:placed + step]
+            cnt = np.bincount((_mix64(keys[:placed + step]) & mask).astype(np.int64),
+                              minlength=1 << log2)
+            linked = int(np.maximum(0, (cnt + 27) // 28 - 1).sum())
+            if linked > cap - 800:
+                break
+            m.put(dev(b), dev(b))
+            o.put(b, b)
+            placed += step
+    used, _ = m.pool_usage()
+    cnt = np.bincount((_mix64(keys[:placed]) & mask).astype(np.int64), minlength=1 << log2)
+    linked = int(np.maximum(0, (cnt + 27) // 28 - 1).sum())
+    assert m.status() == 0
+    assert used == cap, f"cursor not spent ({used} of {cap}); the case is not reached"
+    left = cap - linked
+    assert left >= 500, left
+    new = W.prefill_keys(32, 400)
+    req = (np.full(400, OP_PUT, np.uint8), new, new)
+    srv = Server(m, max_wave_ops=1 << 12, ring_requests=16, arena_ops=1 << 14)
+    srv.start()
+    res, st = _take_all(srv, [req], _submit_all(srv, [req]))
+    srv.stop()
+    srv.close()
+    assert st == [0], "refused although the SM ranges hold enough slabs"
+    assert m.status() == 0
+    want = o.mixed(req[0], req[1], req[2])
+    assert same_results(res[0], want), first_mismatch(res[0], want)
+    assert m.size() == placed + 400
