@@ -26,7 +26,7 @@ _M1 = np.uint64(0xBF58476D1CE4E5B9)
 _M2 = np.uint64(0x94D049BB133111EB)
 VALUE_XOR = 0x9E3779B97F4A7C15
 
-OP_GET, OP_PUT, OP_REMOVE = 0, 1, 2
+OP_GET, OP_PUT, OP_REMOVE, OP_UPDATE = 0, 1, 2, 3
 OP_CONTAINS, OP_INSERT = 0, 1
 
 # stream offsets added to a workload's base seed
@@ -159,6 +159,19 @@ def set_mixed_batch(seed: int, batch: int, n_ops: int, mix=(0.5, 0.4, 0.1),
     if type_sort:
         types, keys = type_sorted(types, keys)
     return MixedBatch(types, keys, None)
+
+
+def perm32(idx: np.ndarray) -> np.ndarray:
+    """Distinct u32 keys: a bijective 32-bit mix of idx (odd multiplies and
+    xor-shifts modulo 2^32), the same function the set sweep applies on the
+    device."""
+    x = np.asarray(idx).astype(np.uint64) & np.uint64(0xFFFFFFFF)
+    m = np.uint64(0xFFFFFFFF)
+    with np.errstate(over="ignore"):
+        x = ((x ^ (x >> np.uint64(16))) * np.uint64(0x7FEB352D)) & m
+        x = ((x ^ (x >> np.uint64(15))) * np.uint64(0x846CA68B)) & m
+        x = x ^ (x >> np.uint64(16))
+    return x.astype(np.uint32)
 
 
 def set_prefill_keys(seed: int, count: int) -> np.ndarray:

@@ -342,17 +342,55 @@ def test_empty_and_bad_arguments(cuda):
 @pytest.mark.parametrize("prefetch", [0, 1, 2])
 @pytest.mark.parametrize("chunk", [0, 2048])
 @pytest.mark.parametrize("split", [0, 100])
-def test_every_tuning_is_exact(cuda, block, prefetch, chunk, split):
-    """Launch tuning never changes results (fused and per-phase paths)."""
+@pytest.mark.parametrize("dedup", [0, 1])
+def test_every_tuning_is_exact(cuda, block, prefetch, chunk, split, dedup):
+    """Launch tuning never changes results (fused and per-phase paths),
+    in-warp deduplication of same-key lookups included."""
     n, log2 = 40_000, 6
     types, keys, vals = _mixed_case(71, n, key_space=1500)
     want = OracleMap(log2).mixed(types, keys, vals)
     for fused in (True, False):
         m = Map(log2, max_window=8192)
-        m.set_tuning(block_threads=block, prefetch=prefetch, chunk=chunk, fused_split=split)
+        m.set_tuning(block_threads=block, prefetch=prefetch, chunk=chunk, fused_split=split,
+                     dedup=dedup)
         out = results_buf(n)
         (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
         _sync()
         got = results(out)
         assert same_results(got, want), f"fused={fused}: " + first_mismatch(got, want)
+        assert m.status() == 0
+
+
+@pytest.mark.parametrize("prefetch", [0, 2])
+def test_dedup_on_hot_keys(cuda, prefetch):
+    """In-warp deduplication (lanes with the same key share one lookup) on a
+    batch where most warps carry repeated keys: a Zipf(1.2) mix over 64 keys
+    with gets, puts and removes interleaved, several windows, reads-only
+    calls too.  Results and final contents equal the oracle's replay, on the
+    fused and the per-phase paths."""
+    rng = np.random.default_rng(83)
+    n, log2 = 200_000, 5
+    ranks = np.minimum(rng.zipf(1.2, size=n) - 1, 63).astype(np.uint64)
+    keys = W.key_of_rank(83, ranks)
+    types = rng.choice([OP_GET, OP_PUT, OP_REMOVE], size=n, p=[0.7, 0.2, 0.1]).astype(np.uint8)
+    vals = rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64)
+    o = OracleMap(log2)
+    want = o.mixed(types, keys, vals)
+    gets = W.key_of_rank(83, np.arange(80, dtype=np.uint64))
+    want_gets = o.get(gets)
+    for fused in (True, False):
+        m = Map(log2, max_window=1 << 15)
+        m.set_tuning(dedup=1, prefetch=prefetch)
+        out = results_buf(n)
+        (m.execute_fused if fused else m.execute)(dev(types), dev(keys), dev(vals), out)
+        g_out = results_buf(len(gets))
+        m.get(dev(gets), g_out)
+        _sync()
+        got = results(out)
+        assert same_results(got, want), f"fused={fused}: " + first_mismatch(got, want)
+        gg = results(g_out)
+        assert same_results(gg, want_gets), first_mismatch(gg, want_gets)
+        k, v = m.dump()
+        ok, ov = o.dump()
+        assert np.array_equal(k, ok) and np.array_equal(v, ov)
         assert m.status() == 0
