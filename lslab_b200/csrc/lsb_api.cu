@@ -42,13 +42,71 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 
 // ------------------------------------------------------------- kernels
 // Every kernel is bounded to 64 registers a thread (launch bound 1024), so any
-// block size from 128 to 1024 threads can reach 2048 threads per SM.
+// block size from 128 to 1024 threads can reach 2048 threads per SM.  The
+// probe and fused kernels' bounds are build settings (blocks of 1024 threads
+// resident per SM: 1 = up to 64 registers a thread, 2 = up to 32).
+#ifndef LSB_PROBE_MIN_BLOCKS
+#define LSB_PROBE_MIN_BLOCKS 1
+#endif
+#ifndef LSB_FUSED_MIN_BLOCKS
+#define LSB_FUSED_MIN_BLOCKS 1
+#endif
 template <class Tr, bool kGroup, int P>
-__global__ void __launch_bounds__(1024, 1)
+__global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
   const uint32_t warp = spread_warp();
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
+}
+
+// Read-only batch (get / contains) in its lean form: one op per thread, no
+// grouping, no work claims, the result written straight out.  The code is
+// kept within 32 registers a thread (launch bound 256 x 8), so 2048 threads
+// fit an SM: a lookup is two dependent loads (meta sector, then the
+// candidate slot), latency-bound, and twice the resident warps keep twice
+// the lookups in flight.  The first candidate is tried inline; a second
+// candidate or a longer chain continues in find_rest.
+template <class Tr>
+__global__ void __launch_bounds__(256, 8)
+    k_read(TableView t, const typename Tr::Key* keys, void* out, uint32_t out_kind, uint32_t n) {
+  using Key = typename Tr::Key;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Key key;
+  if constexpr (sizeof(Key) == 8)
+    key = (Key)ld_cs_u64(keys + i);
+  else
+    key = (Key)ld_cs_u32(keys + i);
+  const uint64_t h = Tr::hash(key);
+  const uint32_t s = (uint32_t)h & t.mask;
+  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
+  const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
+  const Meta m = load_meta<true>(slab);
+  uint32_t cand = tag_match(m, rep);
+  bool found = false;
+  uint64_t val = 0;
+  if (cand) {
+    const int slot = __ffs(cand) - 1;
+    cand &= cand - 1;
+    if constexpr (Tr::kHasValue) {
+      const ulonglong2 kv = ld_ca_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
+      found = kv.x == (uint64_t)key;
+      val = kv.y;
+    } else {
+      found = ld_ca_u32(slab + kMetaBytes + slot * Tr::kSlotBytes) == (uint32_t)key;
+    }
+  }
+  if (!found && (cand || m.next != 0)) {
+    uint64_t loc;
+    found = find_rest<Tr>(t, key, rep, s, m, cand, &val, &loc);
+  }
+  if (out_kind == kOutResult) {
+    uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
+    st_cs_u64(p, found ? 1ull : 0ull);
+    st_cs_u64(p + 1, found ? val : 0ull);
+  } else if (out_kind == kOutBool) {
+    st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+  }
 }
 
 // Ordering of the window's big groups; when hot keys produced groups of
@@ -254,7 +312,7 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
 }
 
 template <class Tr, int P>
-__global__ void __launch_bounds__(1024, 1)
+__global__ void __launch_bounds__(1024, LSB_FUSED_MIN_BLOCKS)
     k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
   uint32_t seq = 0;
@@ -858,9 +916,21 @@ struct Table {
     }
   }
 
-  // Read-only batch: one probe launch per 2^23 ops, no grouping.
+  // Read-only batch: the lean read kernel (k_read), or, with in-warp dedup
+  // or reader locks, the tuned probe kernel (one launch per 2^23 ops, no
+  // grouping).
   int run_reads(const typename Tr::Key* keys, void* out, uint32_t out_kind, size_t n,
                 cudaStream_t s) {
+    if (!tune.dedup && lock_mode != kLockRW) {
+      for (size_t off = 0; off < n; off += (size_t)1 << 30) {
+        const uint32_t m = (uint32_t)std::min<size_t>((size_t)1 << 30, n - off);
+        k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(
+            view(), keys + off, out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr,
+            out ? out_kind : kOutNone, m);
+        LSB_CK(cudaGetLastError());
+      }
+      return LSB_OK;
+    }
     for (size_t off = 0; off < n; off += (size_t)kMaxWindow) {
       uint32_t m = (uint32_t)std::min<size_t>(kMaxWindow, n - off);
       Window<Tr> w = window(nullptr, kOpRead, keys + off, 1, nullptr, 1,
