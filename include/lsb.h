@@ -51,6 +51,7 @@ extern "C" {
 #define LSB_OP_GET 0u
 #define LSB_OP_PUT 1u
 #define LSB_OP_REMOVE 2u
+#define LSB_OP_UPDATE 3u /* map: overwrite a present key's value; an absent key stays absent */
 #define LSB_OP_CONTAINS 0u /* set */
 #define LSB_OP_INSERT 1u   /* set */
 
@@ -130,15 +131,26 @@ int lsb_map_put(lsb_map* m, const uint64_t* keys, const uint64_t* vals, uint64_t
 int lsb_map_put_pairs(lsb_map* m, const lsb_kv* ops, uint64_t* old_out, size_t n,
                       cudaStream_t stream);
 
+/* lslab::map::update<bs>(pair<K,V>*, pair<bool,V>*, size_t, cudaStream_t),
+ * include/lslab/map.h:217-220 -> map_kernels::update_, map_kernels.h:72-89,
+ * with the semantics the reference intends (map.h:154-183, the UPDATE branch
+ * of traverse.h:127-130) and does not deliver (its kernel calls put,
+ * map_kernels.h:85): update-if-present.  out[i] = {1, old value} and the
+ * value becomes ops[i].value when the key is present; {0, 0} and no change
+ * when it is absent.  out may be NULL. */
+int lsb_map_update(lsb_map* m, const lsb_kv* ops, lsb_result* out, size_t n,
+                   cudaStream_t stream);
+
 /* Map remove: the REMOVE branch of detail::traverse
  * (include/lslab/detail/traverse.h:88-91), which the reference map does not
  * expose.  out[i] = {found, old value or 0}; out may be NULL. */
 int lsb_map_remove(lsb_map* m, const uint64_t* keys, lsb_result* out, size_t n,
                    cudaStream_t stream);
 
-/* Mixed batch (types[i] in LSB_OP_GET/PUT/REMOVE), run as internal windows of
- * per-phase launches.  vals is read for puts only and may be NULL when the
- * batch has none.  out[i] as described at lsb_result; may be NULL. */
+/* Mixed batch (types[i] in LSB_OP_GET/PUT/REMOVE/UPDATE), run as internal
+ * windows of per-phase launches.  vals is read for puts and updates only and
+ * may be NULL when the batch has none.  out[i] as described at lsb_result
+ * (an update: {present before it, old value or 0}); may be NULL. */
 int lsb_map_execute(lsb_map* m, const uint8_t* types, const uint64_t* keys,
                     const uint64_t* vals, lsb_result* out, size_t n, cudaStream_t stream);
 

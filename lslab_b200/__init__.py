@@ -6,6 +6,7 @@ Python mirror of the reference's host API (depaulmillz/lslab):
     map.put<bs>(keys, values, old_out, size, stream)   -> Map.put(...)
     map.put<bs>(pairs, old_out, size, stream)          -> Map.put_pairs(...)
     map.get<bs>(keys, pair<bool,V>* out, size, stream) -> Map.get(...)
+    map.update<bs>(pairs, pair<bool,V>* out, size, s)  -> Map.update(...) (update-if-present)
     (REMOVE branch of detail::traverse)                -> Map.remove(...)
     map.buckets()                                      -> Map.buckets()
     lslab::set<K>::set(n_log_2[, Allocator(pool)])      -> Set(n_log_2, pool_slabs)
@@ -22,11 +23,12 @@ import ctypes as C
 
 from . import _lib
 from ._lib import (LOCK_FREE, LOCK_RW, LOCK_WRITER, OP_CONTAINS, OP_GET, OP_INSERT, OP_PUT,
-                   OP_REMOVE, STATUS_BARRIER, STATUS_CHAIN, STATUS_OOM, STATUS_SCRATCH, STATUS_TIMEOUT,
+                   OP_REMOVE, OP_UPDATE, STATUS_BARRIER, STATUS_CHAIN, STATUS_OOM, STATUS_SCRATCH, STATUS_TIMEOUT,
                    LsbError)
 
 __all__ = [
-    "Map", "Set", "Server", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_CONTAINS", "OP_INSERT",
+    "Map", "Set", "Server", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_UPDATE", "OP_CONTAINS",
+    "OP_INSERT",
     "LOCK_WRITER", "LOCK_FREE", "LOCK_RW", "STATUS_OOM", "STATUS_TIMEOUT", "STATUS_CHAIN",
     "STATUS_BARRIER", "STATUS_SCRATCH", "lib",
 ]
@@ -217,6 +219,12 @@ class Map(_Table):
     def put_pairs(self, pairs, output=None, size=None, stream=None):
         n = size if size is not None else (pairs.numel() // 2)
         self._call("put_pairs", _ptr(pairs), _ptr(output), int(n), _stream(stream))
+
+    def update(self, pairs, output=None, size=None, stream=None):
+        """Update-if-present of (key, value) pairs (int64 tensor of shape
+        (n, 2)); output[i] = {present, old value or 0}."""
+        n = size if size is not None else (pairs.numel() // 2)
+        self._call("update", _ptr(pairs), _ptr(output), int(n), _stream(stream))
 
     def remove(self, keys, output=None, size=None, stream=None):
         self._call("remove", _ptr(keys), _ptr(output), _len(keys, size), _stream(stream))

@@ -28,6 +28,7 @@ STATUS_SCRATCH = 0x10
 OP_GET = 0
 OP_PUT = 1
 OP_REMOVE = 2
+OP_UPDATE = 3
 OP_CONTAINS = 0
 OP_INSERT = 1
 
@@ -114,6 +115,7 @@ _SIGS = {
     "lsb_map_put": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
     "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_update": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_execute": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_execute_fused": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_buckets": (_U32, [_P]),

@@ -758,7 +758,7 @@ struct Table {
     void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
                     sc.cnt, sc.obin, sc.perm, sc.clist, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
-                    trace, fused_epoch};
+                    sc.lnu, sc.rnu, trace, fused_epoch};
     for (void* p : ptrs) cudaFree(p);
   }
 
@@ -813,6 +813,8 @@ struct Table {
         cudaMalloc(&sc.hbins, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap) == cudaSuccess &&
         cudaMalloc(&sc.hrun, sizeof(uint32_t) * kHugeBins * (size_t)sc.hcap) == cudaSuccess &&
         cudaMalloc(&sc.runs, sizeof(uint32_t) * 4 * (size_t)sc.rcap) == cudaSuccess &&
+        cudaMalloc(&sc.lnu, sizeof(uint32_t) * window) == cudaSuccess &&
+        cudaMalloc(&sc.rnu, sizeof(uint32_t) * (size_t)sc.rcap) == cudaSuccess &&
         cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess &&
         cudaMalloc(&fused_epoch, sizeof(uint32_t)) == cudaSuccess;
     if (!ok) {
@@ -1376,6 +1378,14 @@ int lsb_map_put_pairs(lsb_map* m, const lsb_kv* ops, uint64_t* old_out, size_t n
   if (n == 0) return LSB_OK;
   const uint64_t* base = reinterpret_cast<const uint64_t*>(ops);
   return m->t.run_plain(nullptr, kOpWrite, base, 2, base + 1, 2, old_out, kOutOld, n, s);
+}
+
+int lsb_map_update(lsb_map* m, const lsb_kv* ops, lsb_result* out, size_t n, cudaStream_t s) {
+  if (!m || (n && !ops)) return LSB_ERR_ARG;
+  if (!aligned(ops, 8) || !aligned(out, 8)) return LSB_ERR_ARG;
+  if (n == 0) return LSB_OK;
+  const uint64_t* base = reinterpret_cast<const uint64_t*>(ops);
+  return m->t.run_plain(nullptr, kOpUpdate, base, 2, base + 1, 2, out, kOutResult, n, s);
 }
 
 int lsb_map_remove(lsb_map* m, const uint64_t* keys, lsb_result* out, size_t n, cudaStream_t s) {

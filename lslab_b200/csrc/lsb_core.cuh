@@ -38,7 +38,9 @@ enum : uint32_t {
   kStatusScratch = 0x10u,
 };
 
-enum : uint8_t { kOpRead = 0, kOpWrite = 1, kOpRemove = 2 };  // get/contains, put/insert, remove
+// get/contains, put/insert, remove, update (map only: overwrite the value of
+// a present key, leave an absent one absent)
+enum : uint8_t { kOpRead = 0, kOpWrite = 1, kOpRemove = 2, kOpUpdate = 3 };
 
 enum : uint32_t { kLockWriter = 0, kLockFree = 1, kLockRW = 2 };
 

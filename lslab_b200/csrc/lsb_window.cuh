@@ -66,7 +66,8 @@ struct WinCounters {
   uint32_t late_cursor;    // next late read handed out in the fused sort pass
   uint32_t huge_count;     // groups with more than kHugeMin members
   uint32_t run_count;      // runs of huge groups (each sorted by one block)
-  uint32_t pad[5];
+  uint32_t upd_count;      // updates among the window's mutations
+  uint32_t pad[4];
 };
 
 __device__ inline void win_counters_reset(WinCounters* c) {
@@ -81,6 +82,7 @@ __device__ inline void win_counters_reset(WinCounters* c) {
   c->tiles_done = 0;
   c->huge_count = 0;
   c->run_count = 0;
+  c->upd_count = 0;
 }
 
 // Scratch owned by a table, sized for max_window ops.
@@ -115,6 +117,11 @@ struct Scratch {
   uint32_t rcap;
   uint32_t* clist;  // compacted mutation indices, clist_cap(max_window) entries
   uint32_t* status; // the table's device status word
+  // windows with updates: an update's effect depends on whether its key is
+  // present just before it, i.e. on the last earlier member of its group
+  // that is not an update
+  uint32_t* lnu;    // per member of a group of > kInline: that member + 1, 0 = none
+  uint32_t* rnu;    // per run of a huge group: 1 + its largest non-update member
 };
 
 enum : uint32_t { kOutNone = 0, kOutResult = 1, kOutOld = 2, kOutBool = 3 };
@@ -369,9 +376,11 @@ __device__ __forceinline__ void probe_ops(const TableView& t, const Scratch& sc,
         const uint32_t first = __reduce_min_sync(0xFFFFFFFFu, is_mut ? i : 0xFFFFFFFFu);
         uint32_t slot_base = 0;
         const uint32_t ldr = __ffs(mm) - 1;
+        const uint32_t um = __ballot_sync(0xFFFFFFFFu, is_mut && type[j] == kOpUpdate);
         if (lane == ldr) {
           slot_base = atomicAdd(&w.cnt->mut_count, (uint32_t)__popc(mm));
           atomicMax(&w.cnt->inv_first_mut, ~first);
+          if (um) atomicAdd(&w.cnt->upd_count, (uint32_t)__popc(um));
         }
         slot_base = __shfl_sync(0xFFFFFFFFu, slot_base, ldr);
         // same-key mutations of this warp join together: the lowest lane
@@ -672,6 +681,69 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
   return warp_base + x - v;
 }
 
+// Block-wide exclusive max-scan of one value per thread (thread order);
+// `tmp` holds one word per warp.  Every thread of the block calls it.
+__device__ __forceinline__ uint32_t block_exclusive_max_scan(uint32_t v, uint32_t* tmp) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t nwarps = (blockDim.x + 31) >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+    if (lane >= (uint32_t)d) x = max(x, y);
+  }
+  const uint32_t excl_in_warp = __shfl_up_sync(0xFFFFFFFFu, x, 1);
+  if (lane == 31) tmp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = lane < nwarps ? tmp[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, d);
+      if (lane >= (uint32_t)d) t = max(t, y);
+    }
+    if (lane < nwarps) tmp[lane] = t;
+  }
+  __syncthreads();
+  uint32_t r = warp ? tmp[warp - 1] : 0;
+  if (lane) r = max(r, excl_in_warp);
+  __syncthreads();
+  return r;
+}
+
+// For the members sorted[0..c) of one group, ascending op indices: each
+// member's lnu = 1 + the last earlier member that is not an update, else
+// `carry` (1 + such a member from before sorted[0], 0 = none).  Chunks of
+// consecutive positions per thread and a block max-scan of the chunks' last
+// non-update member (ascending, so the last is also the largest).  Whole
+// block.
+template <class Tr>
+__device__ void block_lnu(const Scratch& sc, const Window<Tr>& w, const uint32_t* sorted,
+                          uint32_t c, uint32_t carry) {
+  __shared__ uint32_t s_mx[32];
+  const uint32_t per = (c + blockDim.x - 1) / blockDim.x, j0 = threadIdx.x * per;
+  uint32_t last = 0;
+  for (uint32_t k = 0; k < per; ++k) {
+    const uint32_t j = j0 + k;
+    if (j < c) {
+      const uint32_t x = sorted[j];
+      if (x < w.n && op_type(w, x) != kOpUpdate) last = x + 1;
+    }
+  }
+  uint32_t run = max(block_exclusive_max_scan(last, s_mx), carry);
+  for (uint32_t k = 0; k < per; ++k) {
+    const uint32_t j = j0 + k;
+    if (j < c) {
+      const uint32_t x = sorted[j];
+      if (x < w.n) {
+        sc.lnu[x] = run;
+        if (op_type(w, x) != kOpUpdate) run = x + 1;
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // Counting sort of op indices by a bitmap over their range [lo, hi], in
 // passes of kSortChunkWords words; `get(j)` yields member j (< w.n) or an
 // out-of-range value to skip.  Writes the sorted list to seg[off ..].
@@ -748,7 +820,7 @@ __device__ void bitmap_sort(const Scratch& sc, const Window<Tr>& w, uint32_t c, 
 // lookup), so the counting sort reads only shared memory.
 template <class Tr>
 __device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_t gslot,
-                                 uint32_t c, uint32_t off, uint32_t* smem) {
+                                 uint32_t c, uint32_t off, uint32_t* smem, bool upd) {
   uint32_t* sorted = smem + kSortSmall;
   uint32_t* bits = sorted + kSortSmall;
   uint32_t* pre = bits + kSortChunkWords;
@@ -789,6 +861,7 @@ __device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_
     if (e < w.n) sc.pred[e] = p | (j + 1 == c ? kPredLast : 0u);
   }
   __syncthreads();
+  if (upd) block_lnu<Tr>(sc, w, sorted, c, 0u);
 }
 
 // A group of kInline+1 .. kWarpSort members, ordered by one warp: each lane
@@ -796,7 +869,7 @@ __device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_
 // shuffles, tracking its predecessor (the largest smaller index) on the way.
 template <class Tr>
 __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t gslot, uint32_t c,
-                                uint32_t off) {
+                                uint32_t off, bool upd) {
   const uint32_t lane = lane_id();
   uint32_t x[2];
 #pragma unroll
@@ -826,6 +899,25 @@ __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t
       sc.pred[x[g]] = (pred[g] < w.n ? pred[g] + 1 : 0u) | (rank[g] + 1 == c ? kPredLast : 0u);
     }
   }
+  if (!upd) return;  // warp-uniform
+  // lnu: the largest smaller member that is not an update
+  uint32_t nu_of[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    nu_of[h] = (x[h] < w.n && op_type(w, x[h]) != kOpUpdate) ? x[h] : 0xFFFFFFFFu;
+  uint32_t lnu[2] = {0, 0};  // 1 + member, 0 = none
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    for (uint32_t q = 0; q < 32; ++q) {
+      const uint32_t y = __shfl_sync(0xFFFFFFFFu, nu_of[h], q);
+#pragma unroll
+      for (int g = 0; g < 2; ++g)
+        if (y != 0xFFFFFFFFu && y < x[g] && y + 1 > lnu[g]) lnu[g] = y + 1;
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < 2; ++g)
+    if (lane + 32 * g < c && x[g] < w.n) sc.lnu[x[g]] = lnu[g];
 }
 
 // Phase D: block b orders large groups b, b + gridDim.x, ... (the critical
@@ -837,6 +929,7 @@ template <class Tr>
 __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
   __shared__ uint32_t s_off;
   const uint32_t tid = threadIdx.x;
+  const bool upd = ld_cg_u32(&w.cnt->upd_count) != 0;  // settled: the probe has ended
   const uint32_t nlarge = ld_cg_u32(&w.cnt->large_count);
   for (uint32_t job = blockIdx.x; job < nlarge; job += gridDim.x) {
     const uint32_t gslot = ld_cg_u32(&sc.large[job]) & sc.gmask;
@@ -848,7 +941,7 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
     }
     __syncthreads();
     const uint32_t off = s_off;
-    sort_group_block<Tr>(sc, w, gslot, c, off, smem);  // ends with __syncthreads
+    sort_group_block<Tr>(sc, w, gslot, c, off, smem, upd);  // ends with __syncthreads
   }
   const uint32_t nbig = ld_cg_u32(&w.cnt->big_count);
   const uint32_t lane = lane_id(), wpb = blockDim.x >> 5;
@@ -865,7 +958,7 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
       sc.goff[gslot] = off;
     }
     off = __shfl_sync(0xFFFFFFFFu, off, 0);
-    sort_group_warp<Tr>(sc, w, gslot, c, off);
+    sort_group_warp<Tr>(sc, w, gslot, c, off, upd);
   }
 }
 
@@ -1011,6 +1104,7 @@ __device__ void huge_scan(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
           rr[0] = off + p;
           rr[2] = h | (r == 0 ? kRunFirst : 0u) | (r + 1 == nrun ? kRunLast : 0u);
           rr[3] = 0;
+          sc.rnu[base + r] = 0;
         }
         if (r >= 1 && r < nrun && base + r - 1 < sc.rcap)  // the last run ends at total
           sc.runs[4 * (size_t)(base + r - 1) + 1] = off + p;
@@ -1026,6 +1120,7 @@ template <class Tr>
 __device__ void huge_scatter(const Scratch& sc, const Window<Tr>& w, uint32_t gwarp,
                              uint32_t ngwarps) {
   const uint32_t H = huge_groups(sc, w.cnt), width = huge_width(w.n), lane = lane_id();
+  const bool upd = ld_cg_u32(&w.cnt->upd_count) != 0;
   for (uint32_t h = 0; h < H; ++h) {
     uint32_t gslot;
     const uint32_t c = huge_size(sc, w, h, &gslot);
@@ -1047,7 +1142,10 @@ __device__ void huge_scatter(const Scratch& sc, const Window<Tr>& w, uint32_t gw
       if (p < end && p < sc.max_window) {
         sc.seg[p] = x;
         const uint32_t r = ld_cg_u32(&hrun[b]);
-        if (r < sc.rcap) atomicMax(&sc.runs[4 * (size_t)r + 3], x + 1);
+        if (r < sc.rcap) {
+          atomicMax(&sc.runs[4 * (size_t)r + 3], x + 1);
+          if (upd && op_type(w, x) != kOpUpdate) atomicMax(&sc.rnu[r], x + 1);
+        }
       } else {
         raise_status(sc.status, kStatusScratch);
       }
@@ -1064,6 +1162,8 @@ __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
   const uint32_t H = huge_groups(sc, w.cnt);
   for (size_t i = gtid; i < (size_t)H * kHugeBins; i += gthreads) sc.hbins[i] = 0;
   const uint32_t R = min(ld_cg_u32(&w.cnt->run_count), sc.rcap);
+  const bool upd = ld_cg_u32(&w.cnt->upd_count) != 0;
+  __shared__ uint32_t s_carry;
   uint32_t* sorted = smem + kSortSmall;
   uint32_t* bits = sorted + kSortSmall;
   uint32_t* pre = bits + kSortChunkWords;
@@ -1090,6 +1190,22 @@ __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
       if (x < w.n) sc.pred[x] = (pe < w.n ? pe + 1 : 0u) | (last ? kPredLast : 0u);
     }
     __syncthreads();
+    if (upd) {  // block-uniform
+      // carry: the largest non-update member of the nearest earlier run of
+      // the same group that has one (each run's was recorded by the scatter)
+      if (tid == 0) {
+        uint32_t carry = 0, cur = r, cinfo = info;
+        for (uint32_t hop = 0; hop < sc.rcap && !(cinfo & kRunFirst) && cur > 0; ++hop) {
+          --cur;
+          carry = ld_cg_u32(&sc.rnu[cur]);
+          if (carry) break;
+          cinfo = ld_cg_u32(&sc.runs[4 * (size_t)cur + 2]);
+        }
+        s_carry = carry;
+      }
+      __syncthreads();
+      block_lnu<Tr>(sc, w, sorted, n, s_carry);  // ends with __syncthreads
+    }
   }
 }
 
@@ -1123,13 +1239,50 @@ __device__ inline void release_counters(WinCounters* cnt, GridBarrier* bar, void
 }
 
 // ---------------------------------------------------------------- phase E
-// Post-state of mutation p as (present, value).
+// Last member of a small group (inline members only) before op x that is not
+// an update, or 0xFFFFFFFF.
 template <class Tr>
-__device__ __forceinline__ void post_state(const Window<Tr>& w, uint32_t p, bool* present,
+__device__ __noinline__ uint32_t inline_lnu(const Scratch& sc, const Window<Tr>& w, uint32_t gslot,
+                                            uint32_t c, uint32_t x) {
+  uint32_t best = 0xFFFFFFFFu;
+  for (uint32_t q = 0; q < c && q < kInline; ++q) {
+    const uint32_t m = ld_cg_u32(&sc.ginl[(size_t)gslot * kInline + q]);
+    if (m < x && m < w.n && (best == 0xFFFFFFFFu || m > best) && op_type(w, m) != kOpUpdate)
+      best = m;
+  }
+  return best;
+}
+
+// Whether the key of mutation x (group gslot of c members) is present just
+// before x: decided by the last earlier member that is not an update (a put
+// makes it present, a remove absent), else by the window's starting state,
+// which the probe recorded for every member.  Only asked for updates.
+template <class Tr>
+__device__ __forceinline__ bool present_before(const Scratch& sc, const Window<Tr>& w,
+                                               uint32_t gslot, uint32_t c, uint32_t x) {
+  uint32_t l;
+  if (c <= kInline) {
+    l = inline_lnu<Tr>(sc, w, gslot, c, x);
+  } else {
+    const uint32_t e = ld_cg_u32(&sc.lnu[x]);
+    l = e ? e - 1 : 0xFFFFFFFFu;
+  }
+  if (l < w.n) return op_type(w, l) == kOpWrite;
+  return (ld_cg_u64(&sc.mloc[x]) & kLocLive) != 0;
+}
+
+// Post-state of mutation p (group gslot of c members) as (present, value):
+// a put leaves {present, its value}, a remove {absent}, an update its value
+// if the key was present before it and {absent} otherwise.
+template <class Tr>
+__device__ __forceinline__ void post_state(const Scratch& sc, const Window<Tr>& w, uint32_t p,
+                                           uint32_t gslot, uint32_t c, bool* present,
                                            uint64_t* value) {
   const uint8_t pt = op_type(w, p);
-  *present = pt == kOpWrite;
-  *value = (Tr::kHasValue && pt == kOpWrite) ? val_of(w, p) : 0ull;
+  bool pres = pt == kOpWrite;
+  if (pt == kOpUpdate) pres = present_before<Tr>(sc, w, gslot, c, p);
+  *present = pres;
+  *value = (Tr::kHasValue && pres) ? val_of(w, p) : 0ull;
 }
 
 // Inline members of a small group: predecessor of op i (or 0xFFFFFFFF) and
@@ -1177,12 +1330,13 @@ __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
     if (pred < w.n) {
       bool present;
       uint64_t value;
-      post_state(w, pred, &present, &value);
+      post_state<Tr>(sc, w, pred, gslot, c, &present, &value);
       write_result(w, m, type, present, value);
     }
     if (last) {
       const typename Tr::Key key = key_of(w, m);
-      const bool present = type == kOpWrite;
+      bool present = type == kOpWrite;
+      if (type == kOpUpdate) present = present_before<Tr>(sc, w, gslot, c, m);
       const uint64_t val = (Tr::kHasValue && present) ? val_of(w, m) : 0ull;
       table_apply_known<Tr>(t, key, Tr::hash(key), ld_cg_u64(&sc.mloc[m]), present, val);
     }
@@ -1233,7 +1387,7 @@ __device__ void phase_resolve_reads(const Scratch& sc, const Window<Tr>& w, uint
     if (pred_op < w.n) {
       bool present;
       uint64_t value;
-      post_state(w, pred_op, &present, &value);
+      post_state<Tr>(sc, w, pred_op, slot, c, &present, &value);
       write_result(w, i, type, present, value);
     }
   }

@@ -77,6 +77,7 @@ def _olib():
             "orc_map_get": (None, [P, P, P, SZ]),
             "orc_map_put": (None, [P, P, P, P, SZ]),
             "orc_map_remove": (None, [P, P, P, SZ]),
+            "orc_map_update": (None, [P, P, P, P, SZ]),
             "orc_map_mixed": (None, [P, P, P, P, P, SZ]),
             "orc_map_mixed_mt": (C.c_int, [P, P, P, P, P, SZ, C.c_int]),
             "orc_map_size": (SZ, [P]),
@@ -137,6 +138,13 @@ class OracleMap:
         keys = np.ascontiguousarray(keys, np.uint64)
         out = np.zeros(len(keys), RESULT_DTYPE)
         _olib().orc_map_remove(self.h, _p(keys), _p(out), len(keys))
+        return out
+
+    def update(self, keys, vals):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        vals = np.ascontiguousarray(vals, np.uint64)
+        out = np.zeros(len(keys), RESULT_DTYPE)
+        _olib().orc_map_update(self.h, _p(keys), _p(vals), _p(out), len(keys))
         return out
 
     def mixed(self, types, keys, vals=None, threads: int = 1):

@@ -187,6 +187,25 @@ static uint64_t map_upsert(orc_map* m, uint64_t key, uint64_t val, int* existed)
   }
 }
 
+/* UPDATE (the UPDATE branch of traverse.h:127-130 with the functor of
+ * map.h:167-183, which overwrites the value lane of a hit and does nothing on
+ * a miss), reporting the lane's prior value: the reference's functor meant to
+ * (its `tmp` receives the new value instead, map.h:170) and its batched
+ * update_ calls put instead (map_kernels.h:85). */
+static int map_update(orc_map* m, uint64_t key, uint64_t val, uint64_t* old) {
+  map_slab* s = &m->heads[map_bucket(m, key)];
+  for (;;) {
+    int lane = map_match(s, key);
+    if (lane >= 0) {
+      *old = s->value[lane];
+      s->value[lane] = val;
+      return 1;
+    }
+    if (s->next == NO_NEXT) return 0;
+    s = map_at(m, s->next);
+  }
+}
+
 /* REMOVE with the harness functor: report and zero the value lane. */
 static int map_erase(orc_map* m, uint64_t key, uint64_t* old) {
   map_slab* s = &m->heads[map_bucket(m, key)];
@@ -215,6 +234,10 @@ static inline void map_apply(orc_map* m, uint8_t type, uint64_t key, uint64_t va
     uint64_t old = map_upsert(m, key, val, &existed);
     r->found = (uint8_t)existed;
     r->value = old;
+  } else if (type == ORC_UPDATE) {
+    uint64_t old = 0;
+    r->found = (uint8_t)map_update(m, key, val, &old);
+    r->value = r->found ? old : 0;
   } else {
     uint64_t old = 0;
     r->found = (uint8_t)map_erase(m, key, &old);
@@ -234,6 +257,11 @@ void orc_map_put(orc_map* m, const uint64_t* keys, const uint64_t* vals, uint64_
     map_apply(m, ORC_PUT, keys[i], vals[i], &r);
     old_out[i] = r.value;
   }
+}
+
+void orc_map_update(orc_map* m, const uint64_t* keys, const uint64_t* vals, orc_result* out,
+                    size_t n) {
+  for (size_t i = 0; i < n; ++i) map_apply(m, ORC_UPDATE, keys[i], vals[i], &out[i]);
 }
 
 void orc_map_remove(orc_map* m, const uint64_t* keys, orc_result* out, size_t n) {

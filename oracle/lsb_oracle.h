@@ -20,7 +20,7 @@ extern "C" {
 #endif
 
 /* Op codes of a mixed batch (same numbering as the product's lsb.h). */
-enum { ORC_GET = 0, ORC_PUT = 1, ORC_REMOVE = 2 };
+enum { ORC_GET = 0, ORC_PUT = 1, ORC_REMOVE = 2, ORC_UPDATE = 3 };
 enum { ORC_CONTAINS = 0, ORC_INSERT = 1, ORC_SET_REMOVE = 2 };
 
 /* 16-byte result, layout of cuda::std::pair<bool, uint64_t>. */
@@ -39,7 +39,11 @@ void orc_map_get(orc_map* m, const uint64_t* keys, orc_result* out, size_t n);
 void orc_map_put(orc_map* m, const uint64_t* keys, const uint64_t* vals, uint64_t* old_out,
                  size_t n);
 void orc_map_remove(orc_map* m, const uint64_t* keys, orc_result* out, size_t n);
-/* Mixed batch in op-index order; put results report {existed, old value or 0}. */
+/* Update-if-present: {1, old value} and the new value stored, or {0, 0}. */
+void orc_map_update(orc_map* m, const uint64_t* keys, const uint64_t* vals, orc_result* out,
+                    size_t n);
+/* Mixed batch in op-index order (types ORC_GET/PUT/REMOVE/UPDATE); put and
+ * update results report {existed, old value or 0}. */
 void orc_map_mixed(orc_map* m, const uint8_t* types, const uint64_t* keys,
                    const uint64_t* vals, orc_result* out, size_t n);
 /* Same, with ops sharded by bucket over `threads` host threads; each thread

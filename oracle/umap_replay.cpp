@@ -2,7 +2,8 @@
 // batch op stream replayed on std::unordered_map<uint64_t, uint64_t> in
 // op-index order on the host.  Results use the library's conventions: a get
 // gives {found, value or 0}, a put {existed, old value or 0} and then stores
-// the new value, a remove {existed, value or 0} and then erases the key.
+// the new value, a remove {existed, value or 0} and then erases the key, an
+// update {existed, old value or 0} and then stores the new value if it existed.
 //
 // Keys are spread over `shards` maps by a multiplicative hash.  Ops on
 // different keys commute, so a replay in which every shard processes its own
@@ -57,6 +58,8 @@ void apply(std::unordered_map<uint64_t, uint64_t>& m, uint8_t type, uint64_t key
       m.emplace(key, val);
   } else if (type == 2 && had) {
     m.erase(it);
+  } else if (type == 3 && had) {  // update-if-present
+    it->second = val;
   }
 }
 

@@ -75,6 +75,8 @@ inline void alloc_scratch(lsb::Scratch& sc, uint32_t window, uint32_t* status,
   sc.hbins = (uint32_t*)alloc(4ull * kHugeBins * sc.hcap);
   sc.hrun = (uint32_t*)alloc(4ull * kHugeBins * sc.hcap);
   sc.runs = (uint32_t*)alloc(16ull * sc.rcap);
+  sc.lnu = (uint32_t*)alloc(4ull * window);
+  sc.rnu = (uint32_t*)alloc(4ull * sc.rcap);
   sc.status = status;
 }
 

@@ -121,3 +121,56 @@ def test_whole_batch_in_bounds_and_equal_to_oracle(bins, tmp_path, mode, window)
     assert status == 0
     bad = np.nonzero((got["found"] != want["found"]) | (got["value"] != want["value"]))[0]
     assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}"
+
+
+def _update_case(kind: str):
+    """Mixed batches with updates (update-if-present): whether an update
+    takes effect depends on the last earlier put or remove of its key in the
+    batch, so groups of every ordering path are covered: inline (<= 8
+    members), warp (<= 64), block (<= 4096) and hot keys over several runs."""
+    n = 10_000
+    rng = np.random.default_rng(17)
+    if kind == "mixed":
+        t = rng.choice([0, 1, 2, 3], size=n, p=[0.4, 0.2, 0.15, 0.25]).astype(np.uint8)
+        k = W.key_of_rank(4, rng.integers(0, 400, size=n))
+        k[rng.random(n) < 0.45] = np.uint64(77)  # ~2.7k mutations of one key
+    else:  # "update_runs": a hot key whose ops are nearly all updates, with
+        # rare puts and removes, so whole runs of its members carry nothing
+        t = np.full(n, 3, np.uint8)
+        t[rng.random(n) < 0.004] = 1
+        t[rng.random(n) < 0.003] = 2
+        t[rng.random(n) < 0.2] = 0
+        k = W.key_of_rank(6, rng.integers(0, 50, size=n))
+        k[rng.random(n) < 0.7] = np.uint64(91)
+    v = W.splitmix64(19, 0, n)
+    return t, k, v
+
+
+@pytest.mark.parametrize("kind,mode,window", [("mixed", "tiles", 16_384),
+                                               ("mixed", "muts_first", 16_383),
+                                               ("update_runs", "tiles", 16_384)])
+def test_updates_in_bounds_and_equal_to_oracle(bins, tmp_path, kind, mode, window):
+    t, k, v = _update_case(kind)
+    log2 = 6
+    # half of the keys present before the batch: updates of them take effect
+    pre = np.unique(k)[::2]
+    o = OracleMap(log2)
+    o.put(pre, pre ^ np.uint64(5))
+    want = o.mixed(t, k, v)
+    tt = np.concatenate([np.ones(len(pre), np.uint8), t])
+    kk = np.concatenate([pre, k])
+    vv = np.concatenate([pre ^ np.uint64(5), v])
+    path, outp = tmp_path / "ops.bin", tmp_path / "out.bin"
+    _write_window(path, tt, kk, window, vv)
+    pool = (1 << log2) // 4 + 4096
+    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp)]
+                       + ([mode] if mode != "tiles" else []),
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr[-4000:]
+    raw = np.fromfile(outp, np.uint8)
+    got = raw[: 16 * len(kk)].view(np.dtype([("found", "u1"), ("pad", "u1", (7,)), ("value", "<u8")]))
+    got = got[len(pre):]
+    status = int(raw[16 * len(kk):16 * len(kk) + 4].view(np.uint32)[0])
+    assert status == 0
+    bad = np.nonzero((got["found"] != want["found"]) | (got["value"] != want["value"]))[0]
+    assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}"

@@ -106,16 +106,19 @@ def _dict_replay(types, keys, vals):
             d[k] = int(vals[i])
         elif t == W.OP_REMOVE:
             d.pop(k, None)
+        elif t == W.OP_UPDATE and k in d:
+            d[k] = int(vals[i])
     return found, value, d
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_oracle_equals_dict_replay(seed):
-    """Mixed get/put/remove with heavy key reuse: the slab-list oracle gives the
-    same results as a plain dict replayed in index order."""
+    """Mixed get/put/remove/update with heavy key reuse: the slab-list oracle
+    gives the same results as a plain dict replayed in index order (an update
+    changes a present key's value and leaves an absent key absent)."""
     n = 20_000
     rng = np.random.default_rng(seed)
-    types = rng.choice([0, 1, 2], size=n, p=[0.5, 0.35, 0.15]).astype(np.uint8)
+    types = rng.choice([0, 1, 2, 3], size=n, p=[0.4, 0.3, 0.15, 0.15]).astype(np.uint8)
     keys = W.key_of_rank(seed, rng.integers(0, 500, size=n))
     keys[rng.random(n) < 0.05] = np.uint64(0)
     vals = W.splitmix64(seed, 0, n)
@@ -141,7 +144,8 @@ def test_unordered_map_replay_equals_oracle(shards, threads):
     o.put(pk, pv)
     u = UmapReplay(pk, pv, shards=shards)
     for b in range(3):
-        bt = W.map_zipf_batch(seed, b, 1 << 14, 1 << 13, 0.99, (0.6, 0.3, 0.1), type_sort=False)
+        bt = W.map_zipf_batch(seed, b, 1 << 14, 1 << 13, 0.99, (0.5, 0.25, 0.1, 0.15),
+                              type_sort=False)
         want = o.mixed(bt.types, bt.keys, bt.vals)
         dt, got = u.replay(bt.types, bt.keys, bt.vals, threads=threads)
         assert dt >= 0
