@@ -39,6 +39,7 @@ extern "C" {
 #define LSB_ERR_TIMEOUT 3 /* a bounded device wait gave up (lock, barrier) */
 #define LSB_ERR_CUDA 4    /* a CUDA runtime call failed                    */
 #define LSB_ERR_STATE 5   /* call not valid in the object's current state  */
+#define LSB_ERR_IO 6      /* checkpoint file unreadable, unwritable or corrupt */
 
 /* Device status bits (lsb_map_status / lsb_set_status). */
 #define LSB_STATUS_OOM 0x1u
@@ -208,6 +209,22 @@ int lsb_map_size_noalloc(lsb_map* m, uint64_t* count_out, cudaStream_t stream);
  * Synchronises the stream. */
 int lsb_map_dump(lsb_map* m, uint64_t* keys_out, uint64_t* vals_out, size_t cap,
                  uint64_t* count, cudaStream_t stream);
+
+/* ---- checkpoints --------------------------------------------------------
+ * No reference counterpart (lslab has no persistence).  save writes the
+ * table's live entries as records sorted by key (map: u64 key, u64 value;
+ * set: u32 key) after a 56-byte header (magic "LSBCKPT1", version, container,
+ * log2 buckets, key and value bytes, lock mode, pool slabs, record count, and
+ * a checksum of the records); the format does not depend on the slab layout
+ * or bucket count.  load creates a table (the saved shape, or `opt` when not
+ * NULL; a zero opt->pool_slabs takes the saved pool size) and inserts the
+ * records; it returns LSB_ERR_IO for a missing, truncated or corrupt file
+ * (bad magic, version, container, count or checksum) and creates nothing.
+ * Both synchronise `stream`. */
+int lsb_map_save(lsb_map* m, const char* path, cudaStream_t stream);
+int lsb_map_load(const char* path, const lsb_options* opt, lsb_map** out, cudaStream_t stream);
+int lsb_set_save(lsb_set* s, const char* path, cudaStream_t stream);
+int lsb_set_load(const char* path, const lsb_options* opt, lsb_set** out, cudaStream_t stream);
 
 /* ---- set<uint32_t> ---------------------------------------------------
  * Replaces lslab::set<K>::set(n_log_2) (include/lslab/set.h:31-40) and

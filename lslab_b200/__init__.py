@@ -137,6 +137,28 @@ class _Table:
         self._call("size", C.byref(v), _stream(stream))
         return int(v.value)
 
+    def save(self, path, stream=None) -> None:
+        """Write the live entries to a checkpoint file (synchronises)."""
+        self._call("save", str(path).encode(), _stream(stream))
+
+    @classmethod
+    def load(cls, path, pool_slabs: int = 0, *, max_window: int = 0, lock_mode=None,
+             device: int = -1, stream=None):
+        """A new table holding a checkpoint's entries: the saved shape, or
+        the given options (pool_slabs 0 = the saved pool size)."""
+        self = cls.__new__(cls)
+        self._h = None
+        h = C.c_void_p()
+        opts = None
+        if lock_mode is not None or max_window or pool_slabs or device >= 0:
+            opts = C.byref(_opts(pool_slabs, max_window, lock_mode or "writer", device))
+        _lib.check(getattr(lib(), f"lsb_{cls._prefix}_load")(str(path).encode(), opts,
+                                                              C.byref(h), _stream(stream)),
+                   f"lsb_{cls._prefix}_load")
+        self._h = h
+        self.n_log_2 = (self.buckets() - 1).bit_length()
+        return self
+
     def set_trace(self, on: bool = True) -> None:
         self._call("set_trace", int(bool(on)))
 

@@ -18,6 +18,7 @@ LSB_ERR_OOM = 2
 LSB_ERR_TIMEOUT = 3
 LSB_ERR_CUDA = 4
 LSB_ERR_STATE = 5
+LSB_ERR_IO = 6
 
 STATUS_OOM = 0x1
 STATUS_TIMEOUT = 0x2
@@ -116,6 +117,10 @@ _SIGS = {
     "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_update": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_save": (C.c_int, [_P, C.c_char_p, _P]),
+    "lsb_map_load": (C.c_int, [C.c_char_p, _P, _P, _P]),
+    "lsb_set_save": (C.c_int, [_P, C.c_char_p, _P]),
+    "lsb_set_load": (C.c_int, [C.c_char_p, _P, _P, _P]),
     "lsb_map_execute": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_execute_fused": (C.c_int, [_P, _P, _P, _P, _P, _SZ, _P]),
     "lsb_map_buckets": (_U32, [_P]),

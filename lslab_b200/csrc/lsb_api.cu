@@ -13,6 +13,7 @@
 
 #include "lsb.h"
 #include "lsb_core.cuh"
+#include "lsb_internal.h"
 #include "lsb_window.cuh"
 
 using namespace lsb;
@@ -1272,6 +1273,8 @@ void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buc
 }
 
 int lsb_internal_map_device(const lsb_map* m) { return m->t.device; }
+uint32_t lsb_internal_lock_mode_map(const lsb_map* m) { return m->t.lock_mode; }
+uint32_t lsb_internal_lock_mode_set(const lsb_set* s) { return s->t.lock_mode; }
 
 // ------------------------------------------------------------------ serving
 // Host side of the request loop (see k_serve).  One producer may submit while
@@ -1619,6 +1622,7 @@ const char* lsb_error_string(int code) {
     case LSB_ERR_TIMEOUT: return "a bounded device wait gave up";
     case LSB_ERR_CUDA: return "CUDA runtime error";
     case LSB_ERR_STATE: return "invalid state";
+    case LSB_ERR_IO: return "file could not be read or written, or is not a valid checkpoint";
     default: return "unknown error";
   }
 }

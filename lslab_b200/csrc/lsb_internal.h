@@ -10,3 +10,6 @@
 void lsb_internal_map_view(const lsb_map* m, lsb::TableView* view, uint32_t* buckets);
 // CUDA device the map's memory lives on.
 int lsb_internal_map_device(const lsb_map* m);
+// Lock mode a table was created with (LSB_LOCK_*).
+uint32_t lsb_internal_lock_mode_map(const lsb_map* m);
+uint32_t lsb_internal_lock_mode_set(const lsb_set* s);
