@@ -355,8 +355,12 @@ class RefMap:
     __del__ = close
 
     def put(self, keys, vals, old, stream=0):
-        r = _rlib().lref_map_put(self.h, keys.data_ptr(), vals.data_ptr(),
-                                 old.data_ptr() if old is not None else None, keys.numel(), stream)
+        """`old` receives every op's prior value (the reference's put kernel
+        always writes it, so it is required)."""
+        if old is None:
+            raise ValueError("the reference's put needs an output buffer")
+        r = _rlib().lref_map_put(self.h, keys.data_ptr(), vals.data_ptr(), old.data_ptr(),
+                                 keys.numel(), stream)
         assert r == 0, r
 
     def get(self, keys, out, stream=0):

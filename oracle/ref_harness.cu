@@ -142,6 +142,9 @@ int lref_map_put(void* h, const uint64_t* keys, const uint64_t* vals, uint64_t* 
                  size_t n, void* stream) {
   MapT* m = static_cast<MapT*>(h);
   if (n == 0) return 0;
+  // the reference's put kernel stores every op's old value unconditionally
+  // (include/lslab/detail/map_kernels.h:47-49): a null output is refused here
+  if (!keys || !vals || !old_out) return -2;
   m->put<256>(const_cast<uint64_t*>(keys), const_cast<uint64_t*>(vals), old_out, n,
               (cudaStream_t)stream);
   return check(cudaGetLastError());
@@ -150,12 +153,14 @@ int lref_map_put(void* h, const uint64_t* keys, const uint64_t* vals, uint64_t* 
 int lref_map_get(void* h, const uint64_t* keys, void* out, size_t n, void* stream) {
   MapT* m = static_cast<MapT*>(h);
   if (n == 0) return 0;
+  if (!keys || !out) return -2;  // the kernel writes every result
   m->get<256>(const_cast<uint64_t*>(keys), static_cast<cuda::std::pair<bool, uint64_t>*>(out),
               n, (cudaStream_t)stream);
   return check(cudaGetLastError());
 }
 
 int lref_map_remove(void* h, const uint64_t* keys, void* out, size_t n, void* stream) {
+  if (n && (!keys || !out)) return -2;  // the kernel writes every result
   MapT* m = static_cast<MapT*>(h);
   if (n == 0) return 0;
   unsigned blocks = (unsigned)((n + 255) / 256);
@@ -226,18 +231,21 @@ void lref_set_destroy(void* h) {
 
 int lref_set_insert(void* h, const uint32_t* keys, bool* out, size_t n, void* stream) {
   if (n == 0) return 0;
+  if (!keys || !out) return -2;  // the kernel writes every result
   static_cast<SetT*>(h)->insert<256>(keys, out, n, (cudaStream_t)stream);
   return check(cudaGetLastError());
 }
 
 int lref_set_contains(void* h, const uint32_t* keys, bool* out, size_t n, void* stream) {
   if (n == 0) return 0;
+  if (!keys || !out) return -2;  // the kernel writes every result
   static_cast<SetT*>(h)->contains<256>(keys, out, n, (cudaStream_t)stream);
   return check(cudaGetLastError());
 }
 
 int lref_set_remove(void* h, const uint32_t* keys, bool* out, size_t n, void* stream) {
   if (n == 0) return 0;
+  if (!keys || !out) return -2;  // the kernel writes every result
   static_cast<SetT*>(h)->remove<256>(keys, out, n, (cudaStream_t)stream);
   return check(cudaGetLastError());
 }

@@ -75,7 +75,8 @@ def test_cfg1_plain_gets_full_size_three_way(cuda):
     m = Map(log2)
     _map_prefill(m, pk, pv)
     ref = RefMap(log2, ref_map_pool_bound(log2, pk))
-    ref.put(dev(pk), dev(pv), None)
+    ref_old = cuda.empty(nk, dtype=cuda.int64, device="cuda")
+    ref.put(dev(pk), dev(pv), ref_old)
     o = OracleMap(log2)
     o.put(pk, pv)
     want = o.get(q)
