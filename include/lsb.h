@@ -184,12 +184,23 @@ int lsb_map_read_trace(lsb_map* m, uint64_t* out, size_t cap, size_t* count,
  * then clears them. */
 int lsb_map_status(lsb_map* m, uint32_t* flags, cudaStream_t stream);
 
-/* Slabs handed out from the overflow pool so far, and its capacity
- * (synchronises the stream). */
+/* Overflow slabs in use (handed out and not returned by compaction), and
+ * the pool's capacity (synchronises the stream). */
 int lsb_map_pool_usage(lsb_map* m, uint64_t* used, uint64_t* capacity, cudaStream_t stream);
 
 /* Number of live entries (synchronises the stream). */
 int lsb_map_size(lsb_map* m, uint64_t* count, cudaStream_t stream);
+
+/* Compaction, the slab reclamation the reference lacks (its deallocate is a
+ * no-op, include/lslab/detail/device_allocator.h:73, and it reuses no slot
+ * outside a chain's tail slab, include/lslab/detail/traverse.h:54-55).  Each
+ * chain's live entries move into as few slabs as hold them, removed slots
+ * become empty, and the emptied overflow slabs go back to the pool, which
+ * hands them out again before any fresh slab.  (Inserts also reuse removed
+ * slots in place, except in LSB_LOCK_FREE maps.)  Like a mutating call it
+ * must be stream-ordered with every other call on the table.  *freed
+ * (optional; synchronises the stream) receives the slabs returned. */
+int lsb_map_compact(lsb_map* m, uint64_t* freed, cudaStream_t stream);
 
 /* Number of live entries, written to *count_out, a DEVICE word the caller
  * provides, asynchronously on `stream`, without allocating any memory (no
@@ -262,6 +273,7 @@ int lsb_set_read_trace(lsb_set* s, uint64_t* out, size_t cap, size_t* count,
 int lsb_set_status(lsb_set* s, uint32_t* flags, cudaStream_t stream);
 int lsb_set_pool_usage(lsb_set* s, uint64_t* used, uint64_t* capacity, cudaStream_t stream);
 int lsb_set_size(lsb_set* s, uint64_t* count, cudaStream_t stream);
+int lsb_set_compact(lsb_set* s, uint64_t* freed, cudaStream_t stream); /* as lsb_map_compact */
 int lsb_set_dump(lsb_set* s, uint32_t* keys_out, size_t cap, uint64_t* count,
                  cudaStream_t stream);
 

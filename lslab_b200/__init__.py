@@ -137,6 +137,13 @@ class _Table:
         self._call("size", C.byref(v), _stream(stream))
         return int(v.value)
 
+    def compact(self, stream=None) -> int:
+        """Pack every chain and return emptied overflow slabs to the pool;
+        returns the slabs freed (synchronises)."""
+        v = C.c_uint64()
+        self._call("compact", C.byref(v), _stream(stream))
+        return int(v.value)
+
     def save(self, path, stream=None) -> None:
         """Write the live entries to a checkpoint file (synchronises)."""
         self._call("save", str(path).encode(), _stream(stream))

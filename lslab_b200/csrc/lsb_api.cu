@@ -421,9 +421,9 @@ __device__ bool grid_barrier_until(GridBarrier* b, uint32_t nblocks, uint32_t* s
   return ok != 0;
 }
 
-// Slabs the pool can still hand out: what the global cursor has left plus
-// what is left in the per-SM ranges (pool_alloc takes those before it
-// reports OOM).  Whole warp; the result is warp-uniform.
+// Slabs the pool can still hand out: the free stack, what the global cursor
+// has left, and what is left in the per-SM ranges (pool_alloc takes those
+// before it reports OOM).  Whole warp; the result is warp-uniform.
 __device__ uint64_t pool_free_slabs(const TableView& t) {
   const uint32_t lane = threadIdx.x & 31;
   uint64_t left = 0;
@@ -435,7 +435,8 @@ __device__ uint64_t pool_free_slabs(const TableView& t) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) left += __shfl_xor_sync(0xFFFFFFFFu, left, d);
   const uint64_t limit = ld_cg_u64(&t.pool[1]), cursor = ld_cg_u64(&t.pool[0]);
-  return left + (limit > cursor ? limit - cursor : 0);
+  const long long top = (long long)ld_cg_u64(&t.pool[kPoolTop]);
+  return left + (limit > cursor ? limit - cursor : 0) + (top > 0 ? (uint64_t)top : 0);
 }
 
 // Warp 0 of block 0: wait (bounded by idle_ns) for requests, then admit the
@@ -655,6 +656,18 @@ out:
   release_counters(sc.cnt, bar, j.fj.bins, 2 * sizeof(BinCounters) / 4);
 }
 
+// Compaction (lsb_*_compact): one thread per bucket; the free-stack top was
+// clamped to >= 0 by k_pool_clamp just before.
+__global__ void k_pool_clamp(uint64_t* pool) {
+  if ((long long)pool[kPoolTop] < 0) pool[kPoolTop] = 0;
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(256) k_compact(TableView t, uint32_t buckets) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < buckets) compact_bucket<Tr>(t, b);
+}
+
 // Live-entry count and dump: one thread per bucket walks the chain.
 template <class Tr>
 __global__ void k_count(TableView t, uint32_t buckets, unsigned long long* count) {
@@ -730,6 +743,7 @@ struct Table {
   int32_t* locks = nullptr;
   uint32_t* status = nullptr;
   uint64_t* pool = nullptr;
+  uint32_t* free_stack = nullptr;  // slabs returned by compaction (pool_slabs entries)
   GridBarrier* bar = nullptr;
   Scratch sc{};
   uint32_t epoch = 0;  // last epoch handed to a window
@@ -749,6 +763,7 @@ struct Table {
     v.locks = locks;
     v.status = status;
     v.pool = pool;
+    v.free_stack = free_stack;
     v.mask = buckets - 1;
     v.lock_mode = lock_mode;
     v.chunk = chunk;
@@ -756,7 +771,7 @@ struct Table {
   }
 
   void release() {
-    void* ptrs[] = {slabs, locks, status, pool, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
+    void* ptrs[] = {slabs, locks, status, pool, free_stack, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
                     sc.cnt, sc.obin, sc.perm, sc.clist, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
                     sc.lnu, sc.rnu, trace, fused_epoch};
@@ -793,7 +808,9 @@ struct Table {
         cudaMalloc(&slabs, slab_bytes) == cudaSuccess &&
         cudaMalloc(&locks, sizeof(int32_t) * buckets) == cudaSuccess &&
         cudaMalloc(&status, sizeof(uint32_t)) == cudaSuccess &&
-        cudaMalloc(&pool, sizeof(uint64_t) * (2 + kPoolSlots)) == cudaSuccess &&
+        cudaMalloc(&pool, sizeof(uint64_t) * kPoolWords) == cudaSuccess &&
+        cudaMalloc(&free_stack, sizeof(uint32_t) * std::max<uint64_t>(1, pool_slabs)) ==
+            cudaSuccess &&
         cudaMalloc(&sc.gtab, sizeof(uint64_t) * g) == cudaSuccess &&
         cudaMalloc(&sc.ginl, sizeof(uint32_t) * kInline * (size_t)g) == cudaSuccess &&
         cudaMalloc(&sc.ctab, sizeof(uint64_t) * cg) == cudaSuccess &&
@@ -826,7 +843,7 @@ struct Table {
     LSB_CK(cudaMemset(slabs, 0, slab_bytes));
     LSB_CK(cudaMemset(locks, 0, sizeof(int32_t) * buckets));
     LSB_CK(cudaMemset(status, 0, sizeof(uint32_t)));
-    std::vector<uint64_t> p(2 + kPoolSlots, 0);
+    std::vector<uint64_t> p(kPoolWords, 0);
     p[0] = buckets;
     p[1] = (uint64_t)buckets + pool_slabs;
     LSB_CK(cudaMemcpy(pool, p.data(), sizeof(uint64_t) * p.size(), cudaMemcpyHostToDevice));
@@ -1075,13 +1092,32 @@ struct Table {
     return LSB_OK;
   }
 
+  // Slabs out of the pool: handed out by the bump allocator (those parked in
+  // per-SM ranges included) minus those back on the free stack.
   int pool_usage(uint64_t* used, uint64_t* cap, cudaStream_t s) {
-    uint64_t p[2];
+    uint64_t p[2], top = 0;
     LSB_CK(cudaStreamSynchronize(s));
     LSB_CK(cudaMemcpy(p, pool, sizeof(p), cudaMemcpyDeviceToHost));
-    uint64_t u = std::min(p[0], p[1]) - buckets;
+    LSB_CK(cudaMemcpy(&top, pool + kPoolTop, sizeof(top), cudaMemcpyDeviceToHost));
+    const uint64_t on_stack = (long long)top > 0 ? top : 0;
+    const uint64_t u = std::min(p[0], p[1]) - buckets - on_stack;
     if (used) *used = u;
     if (cap) *cap = pool_slabs;
+    return LSB_OK;
+  }
+
+  // Compaction of every chain (see compact_bucket); *freed = slabs returned.
+  int compact(uint64_t* freed, cudaStream_t s) {
+    uint64_t before = 0, after = 0;
+    k_pool_clamp<<<1, 1, 0, s>>>(pool);
+    if (freed) LSB_CK(cudaMemcpyAsync(&before, pool + kPoolTop, 8, cudaMemcpyDeviceToHost, s));
+    k_compact<Tr><<<(buckets + 255) / 256, 256, 0, s>>>(view(), buckets);
+    LSB_CK(cudaGetLastError());
+    if (freed) {
+      LSB_CK(cudaMemcpyAsync(&after, pool + kPoolTop, 8, cudaMemcpyDeviceToHost, s));
+      LSB_CK(cudaStreamSynchronize(s));
+      *freed = after - before;
+    }
     return LSB_OK;
   }
 
@@ -1449,6 +1485,16 @@ int lsb_map_pool_usage(lsb_map* m, uint64_t* used, uint64_t* capacity, cudaStrea
 int lsb_map_size(lsb_map* m, uint64_t* count, cudaStream_t s) {
   if (!m || !count) return LSB_ERR_ARG;
   return m->t.size(count, s);
+}
+
+int lsb_map_compact(lsb_map* m, uint64_t* freed, cudaStream_t s) {
+  if (!m) return LSB_ERR_ARG;
+  return m->t.compact(freed, s);
+}
+
+int lsb_set_compact(lsb_set* p, uint64_t* freed, cudaStream_t s) {
+  if (!p) return LSB_ERR_ARG;
+  return p->t.compact(freed, s);
 }
 
 int lsb_map_dump(lsb_map* m, uint64_t* keys_out, uint64_t* vals_out, size_t cap,

@@ -278,8 +278,9 @@ struct MapTraits {
   static constexpr uint32_t kSlabBytes = 480;
   static constexpr uint32_t kSlotBytes = 16;
   static constexpr bool kHasValue = true;
-  // A dead slot may be reused only by its own key: a lock-free reader that
-  // matched the old key could otherwise read the new key's value.
+  // Without the bucket lock (LSB_LOCK_FREE) a dead slot may be reused only by
+  // its own key: a reader that matched the old key could otherwise read the
+  // new key's value.  Locked inserts reuse any dead slot (scan_chain).
   static constexpr bool kReuseDead = false;
   __device__ static uint64_t hash(Key k) { return mix64(k); }
 };
@@ -300,13 +301,19 @@ struct TableView {
   uint8_t* slabs;      // (buckets + pool) slabs
   int32_t* locks;      // one per bucket (reference encoding: 0 free, -1 writer, >0 readers)
   uint32_t* status;    // device status bits
-  uint64_t* pool;      // [0] global cursor, [1] limit, [2 .. 2+kPoolSlots) per-SM ranges
+  uint64_t* pool;      // [0] global cursor, [1] limit, [2 .. 2+kPoolSlots) per-SM ranges,
+                       // [kPoolTop] free-stack top (signed; <= 0: empty)
+  uint32_t* free_stack;  // slabs returned by compaction, taken before the bump pool
   uint32_t mask;       // buckets - 1
   uint32_t lock_mode;
   uint32_t chunk;      // slabs per per-SM refill (smaller for small pools)
 };
 
 // ------------------------------------------------------------ slab pool
+// Slabs that compaction returned sit on a free stack (zeroed); pool_alloc
+// pops from it before it bumps.  Compaction pushes only while it owns the
+// table, so pops never race a push: a pop that finds the stack empty leaves
+// the top below zero, and the next compaction clamps it back to zero first.
 // Per-SM bump ranges refilled in chunks from one global cursor.  A range is
 // one u64 {end:32 | cur:32}; atomicAdd on it hands out cur.  Exactly one
 // thread sees cur == end when a range is spent: it takes a fresh chunk from
@@ -323,6 +330,8 @@ struct TableView {
 // remainder plus the ranges' leftovers (pool_free_slabs) never sees an OOM
 // within that count.
 constexpr int kPoolSlots = 256;
+constexpr int kPoolTop = 2 + kPoolSlots;
+constexpr int kPoolWords = kPoolTop + 1;
 constexpr uint32_t kPoolChunkMax = 32;
 
 inline __device__ __noinline__ uint32_t pool_alloc_leftover(const TableView& t, uint32_t smid) {
@@ -343,6 +352,10 @@ inline __device__ __noinline__ uint32_t pool_alloc_leftover(const TableView& t, 
 }
 
 __device__ __forceinline__ uint32_t pool_alloc(const TableView& t) {
+  if ((long long)ld_relaxed_u64(&t.pool[kPoolTop]) > 0) {
+    const long long top = (long long)atomicAdd((unsigned long long*)&t.pool[kPoolTop], ~0ull);
+    if (top > 0) return t.free_stack[top - 1];
+  }
   const uint32_t smid = sm_id();
   unsigned long long* range = (unsigned long long*)&t.pool[2 + (smid & (kPoolSlots - 1))];
   const unsigned long long old = atomicAdd(range, 1ull);
@@ -536,7 +549,11 @@ struct ScanResult {
   uint32_t tail;       // last slab of the chain
 };
 
-template <class Tr>
+// kReuse: a dead slot of another key counts as free (the set always; the
+// map only under the bucket lock: a lock-free map reader that matched the
+// old key could otherwise read the new key's value, whereas the batch engine
+// never runs a reader while a locked writer runs).
+template <class Tr, bool kReuse>
 __device__ __forceinline__ bool scan_chain(const TableView& t, typename Tr::Key key, uint64_t h,
                                            ScanResult& r, uint32_t start) {
   const uint32_t fp = fingerprint(h);
@@ -561,7 +578,7 @@ __device__ __forceinline__ bool scan_chain(const TableView& t, typename Tr::Key 
     }
     if (r.free_slot < 0) {
       uint32_t fr = tag_match(m, 0u);  // empty
-      if constexpr (Tr::kReuseDead) {
+      if constexpr (kReuse) {
         // dead tags: nonzero with the top bit clear
 #pragma unroll
         for (int w = 0; w < 7; ++w) {
@@ -601,7 +618,7 @@ __device__ void table_apply_locked(const TableView& t, typename Tr::Key key, uin
   ScanResult r;
   r.found_slot = -1;
   r.free_slot = -1;
-  bool found = scan_chain<Tr>(t, key, h, r, bucket);
+  bool found = scan_chain<Tr, true>(t, key, h, r, bucket);
   if (found) {
     uint8_t* slab = slab_ptr(t.slabs, r.found_slab, Tr::kSlabBytes);
     uint8_t* tagp = slab + 4 + r.found_slot;
@@ -646,7 +663,7 @@ __device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, u
     ScanResult r;
     r.found_slot = -1;
     r.free_slot = -1;
-    bool found = scan_chain<Tr>(t, key, h, r, start);
+    bool found = scan_chain<Tr, Tr::kReuseDead>(t, key, h, r, start);
     if (found) {
       uint8_t* slab = slab_ptr(t.slabs, r.found_slab, Tr::kSlabBytes);
       uint32_t* tw = tag_word(slab, r.found_slot);
@@ -757,6 +774,127 @@ __device__ __forceinline__ void table_apply_known(const TableView& t, typename T
     // writing a neighbouring tag byte of the same word at the same time.
     atomicAnd(tag_word(slab, slot), ~(0x80u << (8 * (slot & 3))));
   }
+}
+
+// ----------------------------------------------------------- compaction
+__device__ __forceinline__ uint32_t live_mask(const Meta& m) {
+  uint32_t mask = 0;
+#pragma unroll
+  for (int w = 0; w < 7; ++w) {
+    // live: top bit set and not the busy marker 0x80
+    const uint32_t x = m.tag[w];
+    const uint32_t busy = __vcmpeq4(x, 0x80808080u);
+    const uint32_t lv = x & ~busy & 0x80808080u;
+    uint32_t b = (lv >> 7) & 0x01010101u;
+    b = b | (b >> 7);
+    b = (b | (b >> 14)) & 0xFu;
+    mask |= b << (4 * w);
+  }
+  return mask;
+}
+
+// Tag words with every non-live byte cleared to empty.
+__device__ __forceinline__ void clear_dead(Meta& m) {
+#pragma unroll
+  for (int w = 0; w < 7; ++w) {
+    const uint32_t x = m.tag[w];
+    const uint32_t busy = __vcmpeq4(x, 0x80808080u);
+    const uint32_t lv = x & ~busy & 0x80808080u;  // top bit of each live byte
+    m.tag[w] = x & ((lv >> 7) * 0xFFu);
+  }
+}
+
+__device__ __forceinline__ void store_meta(uint8_t* slab, const Meta& m) {
+  st_cg_u32(slab, m.next);
+#pragma unroll
+  for (int w = 0; w < 7; ++w) st_cg_u32(slab + 4 + 4 * w, m.tag[w]);
+}
+
+// Compaction of bucket b's chain; the caller owns the whole table (no other
+// kernel uses it).  The chain's live entries move into its first
+// need = ceil(live / kSlots) slabs (entries of later slabs fill the free
+// slots of earlier ones in chain order), every removed slot of the kept
+// slabs becomes empty, and the later slabs are zeroed, unlinked and pushed
+// on the pool's free stack.  One thread per bucket; returns the slabs freed.
+template <class Tr>
+__device__ uint32_t compact_bucket(const TableView& t, uint32_t b) {
+  uint8_t* base = t.slabs;
+  uint32_t live = 0;
+  for (uint32_t s = b, hop = 0; hop < kMaxHops; ++hop) {
+    const Meta m = load_meta(slab_ptr(base, s, Tr::kSlabBytes));
+    live += __popc(live_mask(m));
+    if (m.next == 0) break;
+    s = m.next;
+  }
+  const uint32_t need = live ? (live + kSlots - 1) / kSlots : 1u;
+  // front: the kept slabs, whose free slots take the moved entries
+  uint32_t fs = b;
+  Meta fm = load_meta(slab_ptr(base, fs, Tr::kSlabBytes));
+  clear_dead(fm);
+  uint32_t ffree = ~live_mask(fm) & ((1u << kSlots) - 1u);
+  // back: the slabs from chain position `need` on
+  uint32_t last_kept = b, bs = fm.next;
+  for (uint32_t k = 1; k < need && bs != 0; ++k) {
+    last_kept = bs;
+    bs = ld_cg_u32(slab_ptr(base, bs, Tr::kSlabBytes));
+  }
+  uint32_t freed = 0;
+  while (bs != 0) {
+    uint8_t* bp = slab_ptr(base, bs, Tr::kSlabBytes);
+    const Meta bm = load_meta(bp);
+    for (uint32_t lm = live_mask(bm); lm; lm &= lm - 1) {
+      const int j = __ffs(lm) - 1;
+      // next kept slab with a free slot; the kept slabs have room for every
+      // live entry, so the front never passes last_kept
+      while (ffree == 0 && fs != last_kept) {
+        store_meta(slab_ptr(base, fs, Tr::kSlabBytes), fm);
+        fs = fm.next;
+        fm = load_meta(slab_ptr(base, fs, Tr::kSlabBytes));
+        clear_dead(fm);
+        ffree = ~live_mask(fm) & ((1u << kSlots) - 1u);
+      }
+      if (ffree == 0) {  // cannot happen (see above): keep the chain as it is
+        raise_status(t.status, kStatusScratch);
+        store_meta(slab_ptr(base, fs, Tr::kSlabBytes), fm);
+        return freed;
+      }
+      const int i = __ffs(ffree) - 1;
+      ffree &= ffree - 1;
+      uint8_t* fp = slab_ptr(base, fs, Tr::kSlabBytes);
+      if constexpr (Tr::kHasValue) {
+        const ulonglong2 kv = ld_cg_v2u64(bp + kMetaBytes + j * Tr::kSlotBytes);
+        st_cg_v2u64(fp + kMetaBytes + i * Tr::kSlotBytes, kv.x, kv.y);
+      } else {
+        st_cg_u32(fp + kMetaBytes + i * Tr::kSlotBytes,
+                  ld_cg_u32(bp + kMetaBytes + j * Tr::kSlotBytes));
+      }
+      const uint32_t tag = (bm.tag[j >> 2] >> (8 * (j & 3))) & 0xFFu;
+      fm.tag[i >> 2] = (fm.tag[i >> 2] & ~(0xFFu << (8 * (i & 3)))) | (tag << (8 * (i & 3)));
+    }
+    const uint32_t next = bm.next;
+    for (uint32_t o = 0; o < Tr::kSlabBytes; o += 16) st_cg_v2u64(bp + o, 0ull, 0ull);
+    // the stack holds at most the pool's slabs: each is either linked, on the
+    // stack, or not yet handed out (checked anyway before the store)
+    const unsigned long long at = atomicAdd((unsigned long long*)&t.pool[kPoolTop], 1ull);
+    if (at < t.pool[1] - (uint64_t)t.mask - 1ull)
+      t.free_stack[at] = bs;
+    else
+      raise_status(t.status, kStatusScratch);
+    ++freed;
+    bs = next;
+  }
+  if (fs == last_kept) fm.next = 0;
+  store_meta(slab_ptr(base, fs, Tr::kSlabBytes), fm);
+  // the kept slabs after the front cursor: removed slots become empty
+  for (uint32_t s = fs; s != last_kept;) {
+    s = ld_cg_u32(slab_ptr(base, s, Tr::kSlabBytes));
+    uint8_t* sp = slab_ptr(base, s, Tr::kSlabBytes);
+    Meta m = load_meta(sp);
+    clear_dead(m);
+    if (s == last_kept) m.next = 0;
+    store_meta(sp, m);
+  }
+  return freed;
 }
 
 // -------------------------------------------------------- grid barrier

@@ -11,8 +11,12 @@
 // the mutation list, the probe of its tiles, then a pass over the reads.
 // mode muts_first_binned: the same with the reads probed in table-region
 // order (region counts beside the list, the scatter beside the list probe).
+// mode compact: one-pass probe, and every bucket's chain compacted after each
+// window (lsb_map_compact's step), so later windows run on packed chains and
+// on slabs taken back from the free stack.
 // ops file: u32 n, u32 max_window, n x u8 type, n x u64 key, n x u64 value
-// out file: n x lsb_result (u8 found, 7 pad, u64 value), then u32 status
+// out file: n x lsb_result (u8 found, 7 pad, u64 value), then u32 status,
+// u64 pool cursor, u64 free-stack top
 #include "simt_host.h"
 #include "lsb_window.cuh"
 #include "emu_phases.h"
@@ -34,6 +38,7 @@ int main(int argc, char** argv) {
   }
   const bool binned = argc == 7 && std::strcmp(argv[6], "muts_first_binned") == 0;
   const bool muts_first = binned || (argc == 7 && std::strcmp(argv[6], "muts_first") == 0);
+  const bool compact = argc == 7 && std::strcmp(argv[6], "compact") == 0;
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
   uint32_t n = 0, window = 0;
@@ -60,9 +65,10 @@ int main(int argc, char** argv) {
   t.slabs = (uint8_t*)alloc(((size_t)buckets + pool_slabs) * Tr::kSlabBytes);
   t.locks = (int32_t*)alloc(4ull * buckets);
   t.status = (uint32_t*)alloc(4);
-  t.pool = (uint64_t*)alloc(8ull * (2 + kPoolSlots));
+  t.pool = (uint64_t*)alloc(8ull * kPoolWords);
   t.pool[0] = buckets;
   t.pool[1] = buckets + pool_slabs;
+  t.free_stack = (uint32_t*)alloc(4ull * std::max<uint64_t>(1, pool_slabs));
   t.mask = buckets - 1;
   t.lock_mode = kLockWriter;
   t.chunk = (uint32_t)std::min<uint64_t>(kPoolChunkMax,
@@ -136,11 +142,22 @@ int main(int argc, char** argv) {
         phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
         phase_resolve_reads<Tr>(sc, w, tid, nt);
       });
+    if (compact) {
+      if ((long long)t.pool[kPoolTop] < 0) t.pool[kPoolTop] = 0;  // k_pool_clamp
+      const unsigned cgrid = (buckets + 255) / 256;
+      for (unsigned b = 0; b < cgrid; ++b)
+        emu::run_block(256, b, cgrid, [&] {
+          const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+          if (k < buckets) compact_bucket<Tr>(t, k);
+        });
+    }
   }
   FILE* o = std::fopen(argv[5], "wb");
   if (!o) return 2;
   std::fwrite(out, 16, n, o);
   std::fwrite(t.status, 4, 1, o);
+  std::fwrite(&t.pool[0], 8, 1, o);
+  std::fwrite(&t.pool[kPoolTop], 8, 1, o);
   std::fclose(o);
   std::printf("done status=%#x\n", *t.status);
   return 0;
