@@ -1,0 +1,5 @@
+// The reference's include path <lslab/hash.h> (depaulmillz/lslab,
+// include/lslab/hash.h), mapped onto this library's source-compatible front:
+// callers written against lslab build unchanged with -I include/compat.
+#pragma once
+#include "../lslab_drop_in.h"

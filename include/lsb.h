@@ -74,6 +74,22 @@ typedef struct lsb_kv {
   uint64_t value;
 } lsb_kv;
 
+/* Maps with 32-bit values (lslab::map<K, unsigned>, the shape the reference's
+ * own benchmark uses, benchmark/benchmark.cu:56): results in the layout of
+ * cuda::std::pair<bool, uint32_t> (bool at byte 0, value at 4, 8 bytes) and
+ * AoS inputs in that of cuda::std::pair<uint64_t, uint32_t> (16 bytes). */
+typedef struct lsb_result32 {
+  uint8_t found;
+  uint8_t pad[3];
+  uint32_t value;
+} lsb_result32;
+
+typedef struct lsb_kv32 {
+  uint64_t key;
+  uint32_t value;
+  uint32_t pad;
+} lsb_kv32;
+
 typedef struct lsb_map lsb_map;
 typedef struct lsb_set lsb_set;
 
@@ -141,6 +157,21 @@ int lsb_map_put_pairs(lsb_map* m, const lsb_kv* ops, uint64_t* old_out, size_t n
  * when it is absent.  out may be NULL. */
 int lsb_map_update(lsb_map* m, const lsb_kv* ops, lsb_result* out, size_t n,
                    cudaStream_t stream);
+
+/* The same calls for maps whose values are 32-bit: lslab::map<K, unsigned>'s
+ * get<bs> (include/lslab/map.h:208-211), put<bs> SoA and AoS (map.h:198-201,
+ * 189-192) and update<bs> (map.h:217-220, update-if-present as above).  The
+ * table stores the values zero-extended, so the 64-bit calls read them too;
+ * values above 2^32 - 1 stored through the 64-bit calls come back truncated
+ * here. */
+int lsb_map_get_v32(lsb_map* m, const uint64_t* keys, lsb_result32* out, size_t n,
+                    cudaStream_t stream);
+int lsb_map_put_v32(lsb_map* m, const uint64_t* keys, const uint32_t* vals, uint32_t* old_out,
+                    size_t n, cudaStream_t stream);
+int lsb_map_put_pairs_v32(lsb_map* m, const lsb_kv32* ops, uint32_t* old_out, size_t n,
+                          cudaStream_t stream);
+int lsb_map_update_v32(lsb_map* m, const lsb_kv32* ops, lsb_result32* out, size_t n,
+                       cudaStream_t stream);
 
 /* Map remove: the REMOVE branch of detail::traverse
  * (include/lslab/detail/traverse.h:88-91), which the reference map does not

@@ -117,6 +117,10 @@ _SIGS = {
     "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_update": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_get_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_put_v32": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
+    "lsb_map_put_pairs_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_update_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_compact": (C.c_int, [_P, _P, _P]),
     "lsb_set_compact": (C.c_int, [_P, _P, _P]),
     "lsb_map_save": (C.c_int, [_P, C.c_char_p, _P]),

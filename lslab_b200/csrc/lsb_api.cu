@@ -105,6 +105,8 @@ __global__ void __launch_bounds__(256, 8)
     uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
     st_cs_u64(p, found ? 1ull : 0ull);
     st_cs_u64(p + 1, found ? val : 0ull);
+  } else if (out_kind == kOutResult32) {
+    st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
   } else if (out_kind == kOutBool) {
     st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
   }
@@ -204,11 +206,10 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     w.n = min(job.window, job.base.n - start);
     if (w.types) w.types += start;
     w.keys += (size_t)start * w.kstride;
-    if (w.vals) w.vals += (size_t)start * w.vstride;
-    if (w.out) {
-      size_t esz = w.out_kind == kOutResult ? 16 : (w.out_kind == kOutOld ? 8 : 1);
-      w.out = (uint8_t*)w.out + (size_t)start * esz;
-    }
+    if (w.vals)
+      w.vals = reinterpret_cast<const uint64_t*>(reinterpret_cast<const uint8_t*>(w.vals) +
+                                                 (size_t)start * w.vstride * (w.v32 ? 4 : 8));
+    if (w.out) w.out = (uint8_t*)w.out + (size_t)start * out_bytes(w.out_kind);
     w.epoch = 2 * (f + wi) + 1;
     w.cnt = &sc.cnt[wi & 1];
     // the other counter sets were last read in window wi-1, which has ended
@@ -900,8 +901,9 @@ struct Table {
 
   Window<Tr> window(const uint8_t* types, uint8_t uniform, const typename Tr::Key* keys,
                     uint32_t kstride, const uint64_t* vals, uint32_t vstride, void* out,
-                    uint32_t out_kind, uint32_t n) const {
+                    uint32_t out_kind, uint32_t n, bool v32 = false) const {
     Window<Tr> w;
+    w.v32 = v32 ? 1 : 0;
     w.types = types;
     w.uniform = uniform;
     w.keys = keys;
@@ -916,9 +918,7 @@ struct Table {
     return w;
   }
 
-  static size_t out_elem(uint32_t kind) {
-    return kind == kOutResult ? 16 : (kind == kOutOld ? 8 : 1);
-  }
+  static size_t out_elem(uint32_t kind) { return out_bytes(kind); }
 
   int grid_for(uint32_t n) const {
     const int per_sm = 2048 / (int)tune.block;
@@ -966,15 +966,21 @@ struct Table {
 
   // General batch as per-phase launches, window by window: probe, sort of
   // big groups, resolve.
+  // vals: u64 values, or u32 ones when v32 (vstride counts elements of that width).
   int run_plain(const uint8_t* types, uint8_t uniform, const typename Tr::Key* keys,
                 uint32_t kstride, const uint64_t* vals, uint32_t vstride, void* out,
-                uint32_t out_kind, size_t n, cudaStream_t s) {
+                uint32_t out_kind, size_t n, cudaStream_t s, bool v32 = false) {
     const uint32_t W = sc.max_window;
     for (size_t off = 0; off < n; off += W) {
       uint32_t m = (uint32_t)std::min<size_t>(W, n - off);
+      const uint64_t* v =
+          !vals ? nullptr
+          : v32 ? reinterpret_cast<const uint64_t*>(reinterpret_cast<const uint32_t*>(vals) +
+                                                    off * vstride)
+                : vals + off * vstride;
       Window<Tr> w = window(types ? types + off : nullptr, uniform, keys + off * kstride, kstride,
-                            vals ? vals + off * vstride : nullptr, vstride,
-                            out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr, out_kind, m);
+                            v, vstride, out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr,
+                            out_kind, m, v32);
       int e = next_plain_epoch(s, &w.epoch);
       if (e) return e;
       w.cnt = &sc.cnt[0];
@@ -1425,6 +1431,42 @@ int lsb_map_update(lsb_map* m, const lsb_kv* ops, lsb_result* out, size_t n, cud
   if (n == 0) return LSB_OK;
   const uint64_t* base = reinterpret_cast<const uint64_t*>(ops);
   return m->t.run_plain(nullptr, kOpUpdate, base, 2, base + 1, 2, out, kOutResult, n, s);
+}
+
+// ---- 32-bit values (lslab::map<K, unsigned>)
+int lsb_map_get_v32(lsb_map* m, const uint64_t* keys, lsb_result32* out, size_t n,
+                    cudaStream_t s) {
+  if (!m || (n && !keys)) return LSB_ERR_ARG;
+  if (!aligned(keys, 8) || !aligned(out, 8)) return LSB_ERR_ARG;
+  if (n == 0) return LSB_OK;
+  return m->t.run_reads(keys, out, kOutResult32, n, s);
+}
+
+int lsb_map_put_v32(lsb_map* m, const uint64_t* keys, const uint32_t* vals, uint32_t* old_out,
+                    size_t n, cudaStream_t s) {
+  if (!m || (n && (!keys || !vals))) return LSB_ERR_ARG;
+  if (!aligned(keys, 8) || !aligned(vals, 4) || !aligned(old_out, 4)) return LSB_ERR_ARG;
+  if (n == 0) return LSB_OK;
+  return m->t.run_plain(nullptr, kOpWrite, keys, 1, reinterpret_cast<const uint64_t*>(vals), 1,
+                        old_out, kOutOld32, n, s, true);
+}
+
+int lsb_map_put_pairs_v32(lsb_map* m, const lsb_kv32* ops, uint32_t* old_out, size_t n,
+                          cudaStream_t s) {
+  if (!m || (n && !ops)) return LSB_ERR_ARG;
+  if (!aligned(ops, 8) || !aligned(old_out, 4)) return LSB_ERR_ARG;
+  if (n == 0) return LSB_OK;
+  const uint64_t* base = reinterpret_cast<const uint64_t*>(ops);
+  return m->t.run_plain(nullptr, kOpWrite, base, 2, base + 1, 4, old_out, kOutOld32, n, s, true);
+}
+
+int lsb_map_update_v32(lsb_map* m, const lsb_kv32* ops, lsb_result32* out, size_t n,
+                       cudaStream_t s) {
+  if (!m || (n && !ops)) return LSB_ERR_ARG;
+  if (!aligned(ops, 8) || !aligned(out, 8)) return LSB_ERR_ARG;
+  if (n == 0) return LSB_OK;
+  const uint64_t* base = reinterpret_cast<const uint64_t*>(ops);
+  return m->t.run_plain(nullptr, kOpUpdate, base, 2, base + 1, 4, out, kOutResult32, n, s, true);
 }
 
 int lsb_map_remove(lsb_map* m, const uint64_t* keys, lsb_result* out, size_t n, cudaStream_t s) {

@@ -163,6 +163,10 @@ __device__ __forceinline__ void st_cs_u64(void* p, uint64_t v) {
   asm volatile("st.global.cs.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void st_cs_u32(void* p, uint32_t v) {
+  asm volatile("st.global.cs.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ void st_cs_u8(void* p, uint8_t v) {
   asm volatile("st.global.cs.u8 [%0], %1;" ::"l"(p), "h"((unsigned short)v) : "memory");
 }

@@ -124,13 +124,24 @@ struct Scratch {
   uint32_t* rnu;    // per run of a huge group: 1 + its largest non-update member
 };
 
-enum : uint32_t { kOutNone = 0, kOutResult = 1, kOutOld = 2, kOutBool = 3 };
+// Result arrays: kOutResult {u8 found, pad, u64 value} (16 B), kOutOld u64,
+// kOutBool u8, and for maps with 32-bit values kOutResult32 {u8 found, pad,
+// u32 value} (8 B, the layout of cuda::std::pair<bool, uint32_t>) and
+// kOutOld32 u32.
+enum : uint32_t {
+  kOutNone = 0, kOutResult = 1, kOutOld = 2, kOutBool = 3, kOutResult32 = 4, kOutOld32 = 5
+};
+
+__host__ __device__ constexpr uint32_t out_bytes(uint32_t kind) {
+  return kind == kOutResult ? 16 : kind == kOutOld || kind == kOutResult32 ? 8
+       : kind == kOutOld32 ? 4 : kind == kOutBool ? 1 : 0;
+}
 
 template <class Tr>
 struct Window {
   const uint8_t* types;  // null: every op has type `uniform`
   const typename Tr::Key* keys;
-  const uint64_t* vals;  // map puts
+  const uint64_t* vals;  // map puts and updates (u32 elements when v32)
   void* out;
   uint32_t kstride;      // elements between consecutive keys (2 for AoS pairs)
   uint32_t vstride;      // elements between consecutive values
@@ -138,6 +149,7 @@ struct Window {
   uint32_t epoch;        // 1..65535
   uint8_t uniform;
   uint8_t out_kind;
+  uint8_t v32;           // values are 32-bit (stored zero-extended)
   WinCounters* cnt;
 };
 
@@ -153,6 +165,7 @@ __device__ __forceinline__ typename Tr::Key key_of(const Window<Tr>& w, uint32_t
 
 template <class Tr>
 __device__ __forceinline__ uint64_t val_of(const Window<Tr>& w, uint32_t i) {
+  if (w.v32) return reinterpret_cast<const uint32_t*>(w.vals)[(size_t)i * w.vstride];
   return w.vals[(size_t)i * w.vstride];
 }
 
@@ -184,6 +197,12 @@ __device__ __forceinline__ void write_result(const Window<Tr>& w, uint32_t i, ui
     }
     case kOutOld:
       st_cs_u64((uint64_t*)w.out + i, found ? value : 0ull);
+      break;
+    case kOutResult32:  // one 8-byte store: found in byte 0, the value in bytes 4..7
+      st_cs_u64((uint64_t*)w.out + i, found ? (1ull | (value << 32)) : 0ull);
+      break;
+    case kOutOld32:
+      st_cs_u32((uint32_t*)w.out + i, found ? (uint32_t)value : 0u);
       break;
     case kOutBool:
       st_cs_u8((uint8_t*)w.out + i, (type == kOpWrite) ? 1 : (found ? 1 : 0));

@@ -34,6 +34,7 @@ inline uint64_t ld_cs_u64(const void* p) { return emu_detail::ld<uint64_t>(p); }
 inline uint32_t ld_cs_u32(const void* p) { return emu_detail::ld<uint32_t>(p); }
 inline uint8_t ld_cs_u8(const void* p) { return emu_detail::ld<uint8_t>(p); }
 inline void st_cs_u64(void* p, uint64_t v) { emu_detail::st<uint64_t>(p, v); }
+inline void st_cs_u32(void* p, uint32_t v) { emu_detail::st<uint32_t>(p, v); }
 inline void st_cs_u8(void* p, uint8_t v) { emu_detail::st<uint8_t>(p, v); }
 inline uint32_t ld_acquire_u32(const uint32_t* p) { return __atomic_load_n(p, __ATOMIC_ACQUIRE); }
 inline void st_release_u32(uint32_t* p, uint32_t v) { __atomic_store_n(p, v, __ATOMIC_RELEASE); }
