@@ -16,7 +16,9 @@ Arms:
                    (lsb_map_get then lsb_map_put) on an identical table, results
                    checked bit-identical to the fused path; `e2e`: the fused call
                    with pinned HOST buffers, H2D of the batch and D2H of the
-                   results inside the timed region.
+                   results inside the timed region, consecutive batches
+                   pipelined over a copy-in stream, the compute stream and a
+                   copy-out stream.
   --impl reference lslab's own kernels (map::get / map::put, built for sm_100a
                    from the reference sources into oracle/_ref) on the same
                    workload, per-op-type launches as the reference's API offers.
@@ -401,17 +403,40 @@ def run_ours(args, world, rank, local):
     h_keys = [torch.from_numpy(b.keys.view(np.int64)).pin_memory() for b in batches]
     h_vals = [torch.from_numpy(b.vals.view(np.int64)).pin_memory() for b in batches]
     h_out = torch.empty((n, 2), dtype=torch.int64).pin_memory()
-    s_types = torch.empty(n, dtype=torch.uint8, device="cuda")
-    s_keys = torch.empty(n, dtype=torch.int64, device="cuda")
-    s_vals = torch.empty(n, dtype=torch.int64, device="cuda")
-    s_out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    # Pipelined over three streams and a ring of three buffer sets: batch b's
+    # H2D (copy stream), fused launch (the compute stream, so batches apply
+    # in order) and D2H of its results (a second copy stream) overlap the
+    # neighbouring batches' stages; every step still moves its own inputs in
+    # and its own results out inside the timed region.
+    RING = 3
+    s_types = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(RING)]
+    s_keys = [torch.empty(n, dtype=torch.int64, device="cuda") for _ in range(RING)]
+    s_vals = [torch.empty(n, dtype=torch.int64, device="cuda") for _ in range(RING)]
+    s_out = [torch.empty((n, 2), dtype=torch.int64, device="cuda") for _ in range(RING)]
+    h_outs = [h_out] + [torch.empty((n, 2), dtype=torch.int64).pin_memory()
+                        for _ in range(RING - 1)]
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(RING)]
+    ev_done = [torch.cuda.Event() for _ in range(RING)]
+    ev_out = [torch.cuda.Event() for _ in range(RING)]
+    for e in ev_out:
+        e.record(down)
 
     def e2e_step(b):
-        s_types.copy_(h_types[b], non_blocking=True)
-        s_keys.copy_(h_keys[b], non_blocking=True)
-        s_vals.copy_(h_vals[b], non_blocking=True)
-        fused.execute_fused(s_types, s_keys, s_vals, s_out)
-        h_out.copy_(s_out, non_blocking=True)
+        r = b % RING
+        with torch.cuda.stream(up):
+            up.wait_event(ev_out[r])  # the slot's previous results have left
+            s_types[r].copy_(h_types[b], non_blocking=True)
+            s_keys[r].copy_(h_keys[b], non_blocking=True)
+            s_vals[r].copy_(h_vals[b], non_blocking=True)
+            ev_in[r].record(up)
+        stream.wait_event(ev_in[r])
+        fused.execute_fused(s_types[r], s_keys[r], s_vals[r], s_out[r], stream=stream)
+        ev_done[r].record(stream)
+        with torch.cuda.stream(down):
+            down.wait_event(ev_done[r])
+            h_outs[r].copy_(s_out[r], non_blocking=True)
+            ev_out[r].record(down)
 
     for b in range(args.warmup):
         e2e_step(b)
@@ -420,10 +445,10 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ee0.record(stream)
+    ee0.record(up)
     for s in range(args.steps):
         e2e_step(args.warmup + s)
-    ee1.record(stream)
+    ee1.record(down)
     torch.cuda.synchronize()
     wall_e2e = time.perf_counter() - t0
     barrier(world)
@@ -482,7 +507,9 @@ def run_ours(args, world, rank, local):
         "device_status": st,
         "e2e": {"value": round(e2e_value, 2), "unit": "Mops/s",
                 "h2d_bytes_per_step": int(n * 17), "d2h_bytes_per_step": int(n * 16),
-                "wall_s": round(wall_e2e, 4)},
+                "wall_s": round(wall_e2e, 4),
+                "pipeline": "H2D, fused launch and D2H of consecutive batches on three "
+                            "streams, three buffer sets"},
         "gpu_launches": 1,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -612,25 +639,46 @@ def run_reference(args, world, rank, local):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
 
-    # e2e: host buffers, copies inside the timed region
+    # e2e: host buffers, copies inside the timed region, pipelined exactly as
+    # in our arm (copy-in stream, compute stream, copy-out stream, a ring of
+    # three buffer sets)
+    RING = 3
     h_keys = [torch.from_numpy(b.keys.view(np.int64)).pin_memory() for b in batches]
     h_vals = [torch.from_numpy(b.vals.view(np.int64)).pin_memory() for b in batches]
-    h_out = torch.empty((n, 2), dtype=torch.int64).pin_memory()
-    h_old = torch.empty(n, dtype=torch.int64).pin_memory()
-    s_keys = torch.empty(n, dtype=torch.int64, device="cuda")
-    s_vals = torch.empty(n, dtype=torch.int64, device="cuda")
+    h_out = [torch.empty((n, 2), dtype=torch.int64).pin_memory() for _ in range(RING)]
+    h_old = [torch.empty(n, dtype=torch.int64).pin_memory() for _ in range(RING)]
+    s_keys = [torch.empty(n, dtype=torch.int64, device="cuda") for _ in range(RING)]
+    s_vals = [torch.empty(n, dtype=torch.int64, device="cuda") for _ in range(RING)]
+    r_g = [torch.empty((n, 2), dtype=torch.int64, device="cuda") for _ in range(RING)]
+    r_p = [torch.empty(n, dtype=torch.int64, device="cuda") for _ in range(RING)]
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(RING)]
+    ev_done = [torch.cuda.Event() for _ in range(RING)]
+    ev_out = [torch.cuda.Event() for _ in range(RING)]
+    for e in ev_out:
+        e.record(down)
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
+    e2.record(up)
     for s in range(args.steps):
         b = args.warmup + s
-        s_keys.copy_(h_keys[b], non_blocking=True)
-        s_vals.copy_(h_vals[b], non_blocking=True)
-        step(b, s_keys, s_vals)
+        r = b % RING
         g = n_get[b]
-        h_out[:g].copy_(out_g[:g], non_blocking=True)
-        h_old[: n - g].copy_(out_p[: n - g], non_blocking=True)
-    e3.record(stream)
+        with torch.cuda.stream(up):
+            up.wait_event(ev_out[r])
+            s_keys[r].copy_(h_keys[b], non_blocking=True)
+            s_vals[r].copy_(h_vals[b], non_blocking=True)
+            ev_in[r].record(up)
+        stream.wait_event(ev_in[r])
+        m.get(s_keys[r][:g], r_g[r][:g], stream.cuda_stream)
+        m.put(s_keys[r][g:], s_vals[r][g:], r_p[r][: n - g], stream.cuda_stream)
+        ev_done[r].record(stream)
+        with torch.cuda.stream(down):
+            down.wait_event(ev_done[r])
+            h_out[r][:g].copy_(r_g[r][:g], non_blocking=True)
+            h_old[r][: n - g].copy_(r_p[r][: n - g], non_blocking=True)
+            ev_out[r].record(down)
+    e3.record(down)
     torch.cuda.synchronize()
     e2e_ms = e2.elapsed_time(e3)
     clk = clocks.stop()
@@ -664,7 +712,9 @@ def run_reference(args, world, rank, local):
                          "sample": (f"{args.steps} batches of {n} ops on the GPU (the reference "
                                     "is GPU-only; no host cores do the work)")},
         "e2e": {"value": round(e2e_value, 2), "unit": "Mops/s", "h2d_bytes_per_step": n * 16,
-                "d2h_bytes_per_step": int(statistics.mean(16 * g + 8 * (n - g) for g in n_get))},
+                "d2h_bytes_per_step": int(statistics.mean(16 * g + 8 * (n - g) for g in n_get)),
+                "pipeline": "H2D, get+put launches and D2H of consecutive batches on three "
+                            "streams, three buffer sets"},
         "pool_slabs_used": m.pool_used(),
         "clocks": clk,
     }
