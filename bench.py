@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--soak-s", type=float, default=1.0,
                     help="untimed read-only load before timing so clocks leave idle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-side", action="store_true",
+                    help="headline run: skip the side workloads (plain-small against lslab, "
+                         "uneven batches, serving) whose summaries the line carries")
     ap.add_argument("--cpu-batches", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--lock-mode", default="writer", choices=["writer", "free", "rw"])
@@ -520,8 +523,42 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, batches)
         line["cpu_umap"] = cpu_umap(args, batches)
+    if rank == 0 and world == 1 and not args.no_side:
+        fused.close()
+        plain.close()
+        del q_types, q_keys, q_vals, q_out, d_types, d_keys, d_vals, out_f, out_g, out_p
+        torch.cuda.empty_cache()
+        line.update(side_workloads(args, world, rank, local))
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def side_workloads(args, world, rank, local) -> dict:
+    """Compact summaries of the other benchmark configurations, for the
+    headline line: the plain method at small size against lslab's own get,
+    the uneven-batches stream (fused graph against the per-op-type calls),
+    and the serving loop's latency sweep.  Each runs after the timed headline
+    region, with its own timing."""
+    side = argparse.Namespace(**vars(args))
+    side.steps = 5
+    out = {}
+    ps = run_plain_small(side, world, rank, local)
+    out["plain_small"] = {k: ps.get(k) for k in ("ours_mops", "lslab_mops", "ours_over_lslab",
+                                                  "results_identical", "hit_fraction")}
+    bt = run_batches(side, world, rank, local)
+    out["batches"] = {k: bt.get(k) for k in ("fused_mops", "plain_mops", "fused_over_plain",
+                                              "plain_issue", "plain_python_mops",
+                                              "results_identical", "ops", "batches",
+                                              "device_status")}
+    sv = run_serving(side, world, rank, local)
+    at70 = [p for p in sv["sweep"] if abs(p["load"] - 0.7) < 1e-9]
+    out["serving"] = {
+        "peak_mops": sv["peak_mops"], "wave_ops": sv["wave_ops"],
+        "at_70pct": at70[0] if at70 else None,
+        "p99_us_by_load": {str(p["load"]): p["p99_us"] for p in sv["sweep"]},
+        "loop_state": sv["loop"]["state"], "device_status": sv["device_status"],
+    }
+    return out
 
 
 def cpu_baseline(args, batches):
@@ -769,32 +806,53 @@ def run_batches(args, world, rank, local):
     d_out_g = torch.empty((n, 2), dtype=torch.int64, device="cuda")
     d_out_p = torch.empty(n, dtype=torch.int64, device="cuda")
 
-    def plain_pass():
+    d_out_g2 = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    d_out_p2 = torch.empty(n, dtype=torch.int64, device="cuda")
+
+    def plain_pass(st=None, out_g=d_out_g, out_p=d_out_p):
         for b, (g, p) in enumerate(cnt):
             o = int(offs[b])
             r = int(sizes[b]) - g - p
             if g:
-                plain.get(d_keys[o:o + g], d_out_g[o:o + g])
+                plain.get(d_keys[o:o + g], out_g[o:o + g], stream=st)
             if p:
-                plain.put(d_keys[o + g:o + g + p], d_vals[o + g:o + g + p], d_out_p[o + g:o + g + p])
+                plain.put(d_keys[o + g:o + g + p], d_vals[o + g:o + g + p], out_p[o + g:o + g + p],
+                          stream=st)
             if r:
-                plain.remove(d_keys[o + g + p:o + g + p + r], d_out_g[o + g + p:o + g + p + r])
+                plain.remove(d_keys[o + g + p:o + g + p + r], out_g[o + g + p:o + g + p + r],
+                             stream=st)
 
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
     reps = max(1, args.steps)
-    f_ms, p_ms, identical = [], [], True
+    f_ms, p_ms, pg_ms, identical = [], [], [], True
+    cap = torch.cuda.Stream()
     for rep in range(reps):
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
         e[0].record(stream)
         graph.launch()
         e[1].record(stream)
         e[2].record(stream)
-        plain_pass()
+        plain_pass()  # issued from Python: one ctypes call per op type per batch
         e[3].record(stream)
         torch.cuda.synchronize()
         f_ms.append(e[0].elapsed_time(e[1]))
         p_ms.append(e[2].elapsed_time(e[3]))
+        # the same per-op-type calls captured into one CUDA graph, so the GPU
+        # runs them without host issue gaps (captured afresh for each replay:
+        # a replay runs every captured window once, so no window epoch
+        # repeats).  The plain table takes the stream once more; a key's final
+        # state is its last mutation in the stream, so the contents still
+        # equal the fused table's; results go to separate buffers.
+        pg = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(pg, stream=cap):
+            plain_pass(cap, d_out_g2, d_out_p2)
+        e[4].record(stream)
+        pg.replay()
+        e[5].record(stream)
+        torch.cuda.synchronize()
+        pg_ms.append(e[4].elapsed_time(e[5]))
+        del pg
         if rep == 0:
             # fused results vs the per-type calls of the same batches
             isput = torch.from_numpy(types == 1).cuda()
@@ -808,7 +866,7 @@ def run_batches(args, world, rank, local):
     kp, vp = plain.dump()
     identical = identical and np.array_equal(kf, kp) and np.array_equal(vf, vp)
     graph.close()
-    fm, pm = statistics.median(f_ms), statistics.median(p_ms)
+    fm, pm, pgm = statistics.median(f_ms), statistics.median(p_ms), statistics.median(pg_ms)
     line = {
         "workload": "batches",
         "description": (f"{args.nbatches} mixed batches (lognormal median 512, sigma 1.5), "
@@ -816,17 +874,21 @@ def run_batches(args, world, rank, local):
                         f"buckets prefilled with 2^26 keys"),
         "ops": n, "batches": args.nbatches, "reps": reps,
         "fused_mops": round(n / (fm * 1e-3) / 1e6, 1),
-        "plain_mops": round(n / (pm * 1e-3) / 1e6, 1),
-        "fused_over_plain": round(pm / fm, 2),
-        "fused_ms": [round(x, 3) for x in f_ms], "plain_ms": [round(x, 2) for x in p_ms],
+        "plain_mops": round(n / (pgm * 1e-3) / 1e6, 1),
+        "fused_over_plain": round(pgm / fm, 2),
+        "plain_issue": "per-op-type calls captured in one CUDA graph",
+        "plain_python_mops": round(n / (pm * 1e-3) / 1e6, 1),
+        "fused_ms": [round(x, 3) for x in f_ms], "plain_ms": [round(x, 3) for x in pg_ms],
+        "plain_python_ms": [round(x, 2) for x in p_ms],
         "results_identical": identical, "tuning": tuned,
         "plain_calls_per_pass": int(sum((g > 0) + (p > 0) + (int(sizes[b]) - g - p > 0)
                                         for b, (g, p) in enumerate(cnt))),
         "fused_launches_per_pass": 1,
         "device_status": fused.status() | plain.status(),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    fused.close()
+    plain.close()
+    return line
 
 
 def run_serving(args, world, rank, local):
@@ -883,10 +945,10 @@ def run_serving(args, world, rank, local):
         "wave_ops": args.wave_ops, "peak_mops": round(peak / 1e6, 1),
         "p99_us_at_70pct": at70[0]["p99_us"] if at70 else None,
         "sweep": sweep, "loop": stats, "device_status": m.status(),
-        "pool_slabs_used": m.pool_usage()[0] if hasattr(m, "pool_usage") else None,
+        "pool_slabs_used": m.pool_usage()[0],
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    m.close()
+    return line
 
 
 def _perm32(torch, idx):
@@ -1092,9 +1154,10 @@ def run_plain_small(args, world, rank, local):
         res["ours_over_lslab"] = round(res["ours_mops"] / res["lslab_mops"], 2)
         r.close()
     hits = int(((out_m[:, 0] & 0xFF) != 0).sum())
-    print(json.dumps({"workload": "plain-small", "description": run_plain_small.__doc__.split(";")[0],
-                      "gets": nk, "batch_ops": bn, "reps": reps, "hit_fraction": hits / nk,
-                      **res, "device_status": status}), flush=True)
+    m.close()
+    return {"workload": "plain-small", "description": run_plain_small.__doc__.split(";")[0],
+            "gets": nk, "batch_ops": bn, "reps": reps, "hit_fraction": hits / nk,
+            **res, "device_status": status}
 
 
 def main():
@@ -1103,15 +1166,21 @@ def main():
     if args.impl == "reference":
         run_reference(args, world, rank, local)
     elif args.workload == "batches":
-        run_batches(args, world, rank, local)
+        line = run_batches(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     elif args.workload == "serving":
-        run_serving(args, world, rank, local)
+        line = run_serving(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     elif args.workload == "sets":
         run_sets(args, world, rank, local)
     elif args.workload == "locks":
         run_locks(args, world, rank, local)
     elif args.workload == "plain-small":
-        run_plain_small(args, world, rank, local)
+        line = run_plain_small(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     else:
         run_ours(args, world, rank, local)
     if world > 1:
