@@ -52,6 +52,9 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_FUSED_MIN_BLOCKS
 #define LSB_FUSED_MIN_BLOCKS 1
 #endif
+#ifndef LSB_FUSED_LEAN_READS
+#define LSB_FUSED_LEAN_READS 1
+#endif
 template <class Tr, bool kGroup, int P>
 __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
@@ -78,29 +81,8 @@ __global__ void __launch_bounds__(256, 8)
     key = (Key)ld_cs_u64(keys + i);
   else
     key = (Key)ld_cs_u32(keys + i);
-  const uint64_t h = Tr::hash(key);
-  const uint32_t s = (uint32_t)h & t.mask;
-  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
-  const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
-  const Meta m = load_meta<true>(slab);
-  uint32_t cand = tag_match(m, rep);
-  bool found = false;
-  uint64_t val = 0;
-  if (cand) {
-    const int slot = __ffs(cand) - 1;
-    cand &= cand - 1;
-    if constexpr (Tr::kHasValue) {
-      const ulonglong2 kv = ld_ca_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
-      found = kv.x == (uint64_t)key;
-      val = kv.y;
-    } else {
-      found = ld_ca_u32(slab + kMetaBytes + slot * Tr::kSlotBytes) == (uint32_t)key;
-    }
-  }
-  if (!found && (cand || m.next != 0)) {
-    uint64_t loc;
-    found = find_rest<Tr>(t, key, rep, s, m, cand, &val, &loc);
-  }
+  uint64_t val;
+  const bool found = read_lookup<Tr>(t, key, &val);
   if (out_kind == kOutResult) {
     uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
     st_cs_u64(p, found ? 1ull : 0ull);
@@ -224,6 +206,10 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     // list and the ordering pass: the tuned claim size (split 0 has no other
     // use for it), else one tile per warp
     const uint32_t late_chunk = (split == 0 && job.chunk) ? job.chunk : blockDim.x * P;
+    // the list-first order's reads through the lean one-op-per-thread lookup
+    // (no in-warp dedup, no reader locks, no region order)
+    const bool lean_reads = LSB_FUSED_LEAN_READS && !job.dedup && t.lock_mode != kLockRW &&
+                            !job.binned;
     if (kList && split == 0) {
       // Mutations listed, then probed from the list; while their (latency-
       // bound) chains run, blocks take reads from the same cursor as the sort
@@ -237,6 +223,9 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
       if (job.binned) {
         phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
         perm = sc.perm;
+      } else if (lean_reads) {
+        phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, w.n, &w.cnt->tiles_done,
+                            (listed + 31) / 32);
       } else {
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, late_chunk,
                                   job.dedup != 0, ProbeSel{0, w.n, false}, 0, nullptr,
@@ -265,7 +254,9 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     if (has_big || split < w.n) {
       if (has_big) phase_sort_big<Tr>(sc, w, smem);
       if (has_huge) huge_hist<Tr>(sc, w, warp, nwarps);
-      if (split < w.n)  // claimed, so blocks freed by the sort take more
+      if (split < w.n && lean_reads && split == 0 && perm == nullptr)
+        phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, w.n);
+      else if (split < w.n)  // claimed, so blocks freed by the sort take more
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
                                   late_chunk, job.dedup != 0, ProbeSel{split, w.n, false},
                                   split & ~31u, perm);

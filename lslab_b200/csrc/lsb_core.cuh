@@ -467,6 +467,40 @@ __device__ __forceinline__ bool table_find(const TableView& t, typename Tr::Key 
   return find_rest<Tr>(t, key, rep, s, m, tag_match(m, rep), val, loc);
 }
 
+// The lean single lookup of the read-only paths (k_read, and the fused
+// kernel's read loop): the head meta sector, the first candidate slot inline,
+// the rest of the chain in find_rest.  Few registers: it runs in kernels
+// bounded to 32 a thread.
+template <class Tr>
+__device__ __forceinline__ bool read_lookup(const TableView& t, typename Tr::Key key,
+                                            uint64_t* val) {
+  const uint64_t h = Tr::hash(key);
+  const uint32_t s = (uint32_t)h & t.mask;
+  const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
+  const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
+  const Meta m = load_meta<true>(slab);
+  uint32_t cand = tag_match(m, rep);
+  bool found = false;
+  *val = 0;
+  if (cand) {
+    const int slot = __ffs(cand) - 1;
+    cand &= cand - 1;
+    if constexpr (Tr::kHasValue) {
+      const ulonglong2 kv = ld_ca_v2u64(slab + kMetaBytes + slot * Tr::kSlotBytes);
+      found = kv.x == (uint64_t)key;
+      *val = found ? kv.y : 0ull;
+    } else {
+      found = ld_ca_u32(slab + kMetaBytes + slot * Tr::kSlotBytes) == (uint32_t)key;
+    }
+  }
+  if (!found && (cand || m.next != 0)) {
+    uint64_t loc;
+    found = find_rest<Tr>(t, key, rep, s, m, cand, val, &loc);
+    if (!found) *val = 0;
+  }
+  return found;
+}
+
 // P independent lookups issued together: all head meta sectors first, then
 // all first-candidate slots, so a thread keeps up to P loads in flight.  The
 // rare rest (second candidate, longer chain) falls back to find_rest.

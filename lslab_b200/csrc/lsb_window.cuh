@@ -581,6 +581,37 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
   }
 }
 
+// The reads of [lo, hi) (ops of other types are skipped) with the lean
+// lookup, one op per thread: a block claims blockDim.x * 4 ops at a time
+// from *cursor (relative to lo), so blocks that finish early take more.
+// With stop_at, a block takes no further claim once *stop_at has reached
+// stop_target (the rest is claimed by a later call on the same cursor).
+// Every thread of the block calls it.
+template <class Tr>
+__device__ void phase_read_lean(const TableView& t, const Window<Tr>& w, uint32_t* cursor,
+                                uint32_t lo, uint32_t hi, const uint32_t* stop_at = nullptr,
+                                uint32_t stop_target = 0) {
+  __shared__ uint32_t s_base;
+  const uint32_t chunk = blockDim.x * 4;
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_base = (stop_at != nullptr && ld_cg_u32(stop_at) >= stop_target)
+                   ? 0xFFFFFFFFu
+                   : lo + atomicAdd(cursor, chunk);
+    __syncthreads();
+    const uint32_t c0 = s_base;
+    __syncthreads();  // s_base is rewritten next round
+    if (c0 >= hi || c0 < lo) break;  // block-uniform
+    const uint32_t c1 = min(hi, c0 + chunk);
+    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+      if (op_type(w, i) != kOpRead) continue;
+      uint64_t val;
+      const bool found = read_lookup<Tr>(t, key_stream(w, i), &val);
+      write_result(w, i, kOpRead, found, val);
+    }
+  }
+}
+
 // --------------------------------------------------------- region binning
 // Random probes over a multi-GB table are limited by address translation:
 // measured on B200, random 32-B reads over 4 GB run at ~19 G/s, but at ~48 G/s

@@ -121,16 +121,18 @@ int main(int argc, char** argv) {
           if (binned)
             phase_bin_scatter<Tr>(w, sc.obin, sc.perm, bins);
           else  // reads until every list tile is done, as the fused kernel does
-            phase_probe<Tr, false, 1>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, block, false,
-                                      ProbeSel{0, m, false}, 0, nullptr, &w.cnt->tiles_done,
-                                      (listed + 31) / 32);
+            phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, m, &w.cnt->tiles_done,
+                                (listed + 31) / 32);
         });
       for (unsigned b = 0; b < grid; ++b)
         emu::run_block(block, b, grid, [&] {
           const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
           const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-          phase_probe<Tr, false, 1>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, block, false,
-                                    ProbeSel{0, m, false}, 0, binned ? sc.perm : nullptr);
+          if (binned)
+            phase_probe<Tr, false, 1>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, block, false,
+                                      ProbeSel{0, m, false}, 0, sc.perm);
+          else
+            phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, m);
         });
     }
     emu::sort_window<Tr>(sc, w, num_sms, 256, smem);
