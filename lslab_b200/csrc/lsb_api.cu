@@ -45,7 +45,8 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 // Every kernel is bounded to 64 registers a thread (launch bound 1024), so any
 // block size from 128 to 1024 threads can reach 2048 threads per SM.  The
 // probe and fused kernels' bounds are build settings (blocks of 1024 threads
-// resident per SM: 1 = up to 64 registers a thread, 2 = up to 32).
+// resident per SM: 1 = up to 64 registers a thread, 2 = up to 32; or, for the
+// fused kernel, LSB_FUSED_MAXNREG registers a thread at any block size).
 #ifndef LSB_PROBE_MIN_BLOCKS
 #define LSB_PROBE_MIN_BLOCKS 1
 #endif
@@ -304,8 +305,13 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
   }
 }
 
+#ifdef LSB_FUSED_MAXNREG
+#define LSB_FUSED_BOUNDS __maxnreg__(LSB_FUSED_MAXNREG)
+#else
+#define LSB_FUSED_BOUNDS __launch_bounds__(1024, LSB_FUSED_MIN_BLOCKS)
+#endif
 template <class Tr, int P>
-__global__ void __launch_bounds__(1024, LSB_FUSED_MIN_BLOCKS)
+__global__ void LSB_FUSED_BOUNDS
     k_fused(TableView t, Scratch sc, FusedJob<Tr> job, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
   uint32_t seq = 0;

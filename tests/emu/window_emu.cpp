@@ -14,6 +14,8 @@
 // mode compact: one-pass probe, and every bucket's chain compacted after each
 // window (lsb_map_compact's step), so later windows run on packed chains and
 // on slabs taken back from the free stack.
+// mode lockfree: one-pass probe, writers without bucket locks (CAS on slab
+// words, LSB_LOCK_FREE).
 // ops file: u32 n, u32 max_window, n x u8 type, n x u64 key, n x u64 value
 // out file: n x lsb_result (u8 found, 7 pad, u64 value), then u32 status,
 // u64 pool cursor, u64 free-stack top
@@ -39,6 +41,7 @@ int main(int argc, char** argv) {
   const bool binned = argc == 7 && std::strcmp(argv[6], "muts_first_binned") == 0;
   const bool muts_first = binned || (argc == 7 && std::strcmp(argv[6], "muts_first") == 0);
   const bool compact = argc == 7 && std::strcmp(argv[6], "compact") == 0;
+  const bool lockfree = argc == 7 && std::strcmp(argv[6], "lockfree") == 0;
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
   uint32_t n = 0, window = 0;
@@ -70,7 +73,7 @@ int main(int argc, char** argv) {
   t.pool[1] = buckets + pool_slabs;
   t.free_stack = (uint32_t*)alloc(4ull * std::max<uint64_t>(1, pool_slabs));
   t.mask = buckets - 1;
-  t.lock_mode = kLockWriter;
+  t.lock_mode = lockfree ? kLockFree : kLockWriter;
   t.chunk = (uint32_t)std::min<uint64_t>(kPoolChunkMax,
                                          std::max<uint64_t>(1, pool_slabs / (8ull * num_sms)));
   Scratch sc;

@@ -29,6 +29,7 @@ def test_map_save_load_round_trip(cuda, tmp_path):
     m = Map(log2, 1 << 14, lock_mode="free")
     m.put(dev(k), dev(v))
     m.remove(dev(k[::5]))
+    assert m.status() == 0
     path = tmp_path / "m.ck"
     m.save(path)
     host = CK.read(path)

@@ -218,3 +218,34 @@ def test_compaction_between_windows_in_bounds_and_reclaims(bins, tmp_path):
     # run, and the last compaction left emptied slabs on the free stack
     assert bumped < inserted // 28 // 2, (bumped, inserted)
     assert top > 0, top
+
+
+def test_lock_free_inserts_race_without_losing_keys_or_slabs(bins, tmp_path):
+    """LSB_LOCK_FREE writers (CAS on tag and link words) inserting thousands
+    of distinct keys into 8 buckets in one window, on concurrent host
+    threads: every key lands (results and a later read equal the oracle),
+    and chains grow by about one slab per 28 keys (a thread that loses a
+    link race keeps its slab and appends it instead of dropping it)."""
+    log2, n = 3, 6000
+    keys = W.prefill_keys(61, n)
+    t = np.concatenate([np.ones(n, np.uint8), np.zeros(n, np.uint8)])
+    k = np.concatenate([keys, keys])
+    v = np.concatenate([keys ^ np.uint64(9), np.zeros(n, np.uint64)])
+    window = n  # the inserts in one window, the reads in the next
+    path, outp = tmp_path / "ops.bin", tmp_path / "out.bin"
+    _write_window(path, t, k, window, v)
+    want = OracleMap(log2).mixed(t, k, v)
+    pool = 4096
+    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp),
+                        "lockfree"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr[-4000:]
+    raw = np.fromfile(outp, np.uint8)
+    m = len(k)
+    got = raw[: 16 * m].view(np.dtype([("found", "u1"), ("pad", "u1", (7,)), ("value", "<u8")]))
+    status = int(raw[16 * m:16 * m + 4].view(np.uint32)[0])
+    cursor = int(raw[16 * m + 4:16 * m + 12].view(np.uint64)[0])
+    assert status == 0
+    bad = np.nonzero((got["found"] != want["found"]) | (got["value"] != want["value"]))[0]
+    assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}"
+    needed = n // 28 - (1 << log2)  # overflow slabs of perfectly packed chains
+    assert cursor - (1 << log2) <= needed + 2 * (1 << log2) + 64, (cursor, needed)

@@ -394,3 +394,23 @@ def test_dedup_on_hot_keys(cuda, prefetch):
         ok, ov = o.dump()
         assert np.array_equal(k, ok) and np.array_equal(v, ov)
         assert m.status() == 0
+
+
+def test_lock_free_inserts_do_not_waste_slabs(cuda):
+    """LSB_LOCK_FREE map, 200k distinct keys into 256 buckets in one call:
+    many inserts race to grow each chain; none is lost and the pool use stays
+    near one slab per 28 keys (racing inserts keep and append their slabs)."""
+    log2, n = 8, 200_000
+    keys = W.prefill_keys(67, n)
+    needed = n // 28 - (1 << log2)
+    m = Map(log2, needed + 3000, lock_mode="free")
+    m.put(dev(keys), dev(keys))
+    assert m.status() == 0
+    assert m.size() == n
+    used, _ = m.pool_usage()
+    assert used <= needed + 2 * (1 << log2) + 1500, (used, needed)
+    o = OracleMap(log2)
+    o.put(keys, keys)
+    k, v = m.dump()
+    ok, ov = o.dump()
+    assert np.array_equal(k, ok) and np.array_equal(v, ov)

@@ -14,7 +14,7 @@ from lslab_b200 import Map, Server, OP_GET, OP_PUT, OP_REMOVE
 from lslab_b200 import _lib
 from lslab_b200 import workload as W
 from oracle import OracleMap
-from tests.util import same_results, first_mismatch
+from tests.util import dev, same_results, first_mismatch
 
 pytestmark = pytest.mark.gpu
 
