@@ -421,6 +421,26 @@ typedef struct lsb_serve_load {
 int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* load, uint64_t* latency_ns,
                        uint64_t* wall_ns);
 
+/* ---- device per-warp API -------------------------------------------------
+ * The device methods of the reference (map::get/put/update, map.h:92-183;
+ * set::contains/insert/remove, set.h:64-90) are in include/lsb_device.cuh,
+ * used from a caller's own kernels on a view of a table's device memory.
+ * The view is plain data: pass it to kernels by value.  It stays valid until
+ * the table is destroyed. */
+typedef struct lsb_table_view {
+  void* slabs;
+  int32_t* locks;
+  uint32_t* status;
+  uint64_t* pool;
+  uint32_t* free_stack;
+  uint32_t mask;
+  uint32_t lock_mode;
+  uint32_t chunk;
+  uint32_t pad;
+} lsb_table_view;
+int lsb_map_device_view(const lsb_map* m, lsb_table_view* out);
+int lsb_set_device_view(const lsb_set* s, lsb_table_view* out);
+
 /* ---- misc ------------------------------------------------------------- */
 const char* lsb_error_string(int code);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */

@@ -117,6 +117,8 @@ _SIGS = {
     "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_update": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_map_device_view": (C.c_int, [_P, _P]),
+    "lsb_set_device_view": (C.c_int, [_P, _P]),
     "lsb_map_get_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_put_v32": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
     "lsb_map_put_pairs_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),

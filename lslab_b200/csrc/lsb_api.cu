@@ -1364,6 +1364,23 @@ T* dev_ptr(T* host) {
 }
 }  // namespace
 
+// Device view of a table for the per-warp device API (lsb_*_device_view).
+namespace {
+template <class Tr>
+void fill_view(const Table<Tr>& t, lsb_table_view* out) {
+  const TableView v = t.view();
+  out->slabs = v.slabs;
+  out->locks = v.locks;
+  out->status = v.status;
+  out->pool = v.pool;
+  out->free_stack = v.free_stack;
+  out->mask = v.mask;
+  out->lock_mode = v.lock_mode;
+  out->chunk = v.chunk;
+  out->pad = 0;
+}
+}  // namespace
+
 extern "C" {
 
 // ------------------------------------------------------------------ map
@@ -1695,6 +1712,19 @@ int lsb_graph_destroy(lsb_graph* g) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
   delete g;
+  return LSB_OK;
+}
+
+// ------------------------------------------------------ device per-warp API
+int lsb_map_device_view(const lsb_map* m, lsb_table_view* out) {
+  if (!m || !out) return LSB_ERR_ARG;
+  fill_view(m->t, out);
+  return LSB_OK;
+}
+
+int lsb_set_device_view(const lsb_set* s, lsb_table_view* out) {
+  if (!s || !out) return LSB_ERR_ARG;
+  fill_view(s->t, out);
   return LSB_OK;
 }
 
