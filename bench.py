@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="zipf9505",
-                    choices=["zipf9505", "batches", "serving", "sets", "locks", "plain-small"],
+                    choices=["zipf9505", "batches", "serving", "sets", "locks", "plain-small",
+                             "probes"],
                     help="zipf9505: the headline line; batches: 4096 uneven mixed batches in "
                          "one graph-captured fused launch vs per-op-type calls; serving: the "
                          "request loop under open-loop Poisson load")
@@ -1037,6 +1038,83 @@ def run_sets(args, world, rank, local):
                           "batch_ops": n, "steps": args.steps, "points": points}), flush=True)
 
 
+def run_probes(args, world, rank, local):
+    """Probe comparison on read-only batches: the thread-per-op tag probe
+    (default: a 32-B meta sector, then the candidate slot) against the
+    warp-cooperative slab probe of the reference's design (tuning
+    warp_probe=1: a warp serves its lanes' distinct keys one at a time,
+    lanes reading a slab's slots together).  The headline map (2^22 buckets,
+    2^26 keys, the gets of 2^20-op 95/5 Zipf batches) and sets at 1 key per
+    head-slab slot (2^18 and 2^22 buckets, 2^18-op contains batches, half
+    present); same inputs and results checked identical."""
+    import torch
+    import lslab_b200 as L
+    from lslab_b200 import workload as W
+    from lslab_b200.shard import rank_seed
+
+    seed = rank_seed(args.seed, rank)
+    reps = max(3, args.steps)
+
+    def timed(fn, inputs, out):
+        for x in inputs[:2]:
+            fn(x, out)
+        torch.cuda.synchronize()
+        ts = []
+        for x in inputs[2:2 + reps]:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(x, out)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    points = []
+    pk, pv = prefill_arrays(args, rank)
+    m = L.Map(args.buckets_log2, max(1 << (args.buckets_log2 - 2), 4096))
+    for off in range(0, len(pk), 1 << 24):
+        m.put(dev_u64(torch, pk[off:off + (1 << 24)]), dev_u64(torch, pv[off:off + (1 << 24)]))
+    batches = make_batches(args, rank, reps + 2)
+    gets = [dev_u64(torch, b.keys[b.types == 0]) for b in batches]
+    n = max(int(g.numel()) for g in gets)
+    res = {}
+    for wp in (0, 1):
+        m.set_tuning(warp_probe=wp)
+        out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+        ms = timed(lambda k, o: m.get(k, o[:k.numel()]), gets, out)
+        res[wp] = (ms, out[:gets[-1].numel()].clone())
+    same = bool(torch.equal(res[0][1], res[1][1]))
+    points.append({"table": f"map 2^{args.buckets_log2} buckets, 2^{args.prefill_log2} keys",
+                   "ops": int(gets[2].numel()), "tag_probe_us": round(res[0][0] * 1e3, 1),
+                   "warp_probe_us": round(res[1][0] * 1e3, 1),
+                   "tag_over_warp": round(res[1][0] / res[0][0], 2), "results_identical": same})
+    m.close()
+    del gets
+    for log2 in (18, 22):
+        nk = (1 << log2) * 28
+        st = L.Set(log2, nk // 28 + 4096)
+        for off in range(0, nk, 1 << 24):
+            st.insert(_perm32(torch, torch.arange(off, min(nk, off + (1 << 24)), device="cuda")))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed + log2)
+        qs = [_perm32(torch, torch.randint(0, 2 * nk, (1 << 18,), device="cuda", generator=gen))
+              for _ in range(reps + 2)]
+        r = {}
+        for wp in (0, 1):
+            st.set_tuning(warp_probe=wp)
+            out = torch.empty(1 << 18, dtype=torch.bool, device="cuda")
+            ms = timed(lambda k, o: st.contains(k, o), qs, out)
+            r[wp] = (ms, out.clone())
+        points.append({"table": f"set 2^{log2} buckets, 1 key per head slot", "ops": 1 << 18,
+                       "tag_probe_us": round(r[0][0] * 1e3, 1),
+                       "warp_probe_us": round(r[1][0] * 1e3, 1),
+                       "tag_over_warp": round(r[1][0] / r[0][0], 2),
+                       "results_identical": bool(torch.equal(r[0][1], r[1][1]))})
+        st.close()
+    return {"workload": "probes", "description": run_probes.__doc__.split(":")[0],
+            "reps": reps, "points": points}
+
+
 def run_locks(args, world, rank, local):
     """Bucket-lock comparison on the map (writer lock = the reference's
     warp_mutex role; lock-free = CAS on slab tag words; rw = reader-writer
@@ -1177,6 +1255,10 @@ def main():
         run_sets(args, world, rank, local)
     elif args.workload == "locks":
         run_locks(args, world, rank, local)
+    elif args.workload == "probes":
+        line = run_probes(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     elif args.workload == "plain-small":
         line = run_plain_small(args, world, rank, local)
         if rank == 0:

@@ -116,6 +116,10 @@ typedef struct lsb_tuning {
                              while blocks take reads, the remaining reads run during the
                              ordering (faster on batches with interleaved op types) */
   uint32_t region_order;  /* fused path: 1 = probe a window in table-region order */
+  uint32_t warp_probe;    /* read-only batches: 1 = the warp-cooperative slab probe (a
+                             warp serves its lanes' distinct keys one at a time, lanes
+                             reading a slab's slots together); 0 = one op per thread,
+                             tag sector then candidate slot (default, faster) */
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */
@@ -327,10 +331,10 @@ int lsb_graph_launch(lsb_graph* g, cudaStream_t stream);
 int lsb_graph_destroy(lsb_graph* g);
 
 /* Autotuner: times the fused path on a sample batch for every block size
- * (256, 512, 1024 threads = 8, 16, 32 warps), lookahead (0, 1, 2) and probe
- * order: mutations listed and probed first, reads meanwhile and after, with
- * a read claim size of one tile per warp, 2048, 4096, 8192 or 16384 ops; or
- * all ops in one pass with claim size static, 1024, 2048 or 4096 ops.  It
+ * (128, 256, 512, 1024 threads = 4, 8, 16, 32 warps), lookahead (0, 1, 2)
+ * and probe order: mutations listed and probed first, reads meanwhile and
+ * after; or all ops in one pass with the probe's claim size static, 32, 128,
+ * 512, 1024, 2048 or 4096 ops; the median of three timings each.  It
  * keeps the fastest on the table
  * and in a process-wide cache by table size that tables created later with
  * the same log2_buckets start from.  The sample is applied once per

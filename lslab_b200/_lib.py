@@ -61,6 +61,7 @@ class Tuning(C.Structure):
         ("dedup", C.c_uint32),
         ("fused_split", C.c_uint32),
         ("region_order", C.c_uint32),
+        ("warp_probe", C.c_uint32),
     ]
 
 

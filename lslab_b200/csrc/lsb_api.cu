@@ -95,6 +95,82 @@ __global__ void __launch_bounds__(256, 8)
   }
 }
 
+// Read-only batch through the warp-cooperative probe of the reference's
+// design (include/lslab/detail/traverse.h:39-96), kept as a measured
+// alternative to k_read: each warp serves the distinct keys of its 32 lanes
+// one at a time (lanes with the same key share one lookup, found with
+// __match_any_sync); for every slab of the chain, lane l < kSlots reads
+// slot l's tag and its key and value together (the warp reads the slab's
+// whole key area, 14 sectors, plus the meta sector), and __ballot_sync finds
+// the match.  k_read reads 2 sectors per hit instead.
+template <class Tr>
+__global__ void __launch_bounds__(256)
+    k_read_coop(TableView t, const typename Tr::Key* keys, void* out, uint32_t out_kind,
+                uint32_t n) {
+  using Key = typename Tr::Key;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool active = i < n;
+  const Key key = active ? keys[i] : (Key)0;
+  const uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key) & act;
+  const uint32_t leader = active ? (uint32_t)__ffs(peers) - 1 : lane;
+  uint32_t todo = __ballot_sync(0xFFFFFFFFu, active && leader == lane);
+  bool my_found = false;
+  uint64_t my_val = 0;
+  while (todo) {  // warp-uniform
+    const uint32_t src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const Key k = __shfl_sync(0xFFFFFFFFu, key, src);
+    const uint64_t h = Tr::hash(k);
+    const uint32_t live = 0x80u | fingerprint(h);
+    uint32_t s = (uint32_t)h & t.mask;
+    bool found = false;
+    uint64_t val = 0;
+    for (uint32_t hop = 0; hop < kMaxHops; ++hop) {
+      const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
+      bool match = false;
+      uint64_t v = 0;
+      if (lane < (uint32_t)kSlots) {
+        const uint32_t tw = ld_ca_u32(slab + 4 + 4 * (lane >> 2));
+        const uint32_t tag = (tw >> (8 * (lane & 3))) & 0xFFu;
+        if constexpr (Tr::kHasValue) {
+          const ulonglong2 kv = ld_ca_v2u64(slab + kMetaBytes + lane * Tr::kSlotBytes);
+          match = tag == live && kv.x == (uint64_t)k;
+          v = kv.y;
+        } else {
+          match = tag == live && ld_ca_u32(slab + kMetaBytes + lane * Tr::kSlotBytes) == (uint32_t)k;
+        }
+      }
+      const uint32_t next = ld_ca_u32(slab);
+      const uint32_t hit = __ballot_sync(0xFFFFFFFFu, match);
+      if (hit) {
+        found = true;
+        val = __shfl_sync(0xFFFFFFFFu, v, __ffs(hit) - 1);
+        break;
+      }
+      if (next == 0) break;
+      s = next;
+    }
+    if (lane == src) {
+      my_found = found;
+      my_val = val;
+    }
+  }
+  const bool found = __shfl_sync(0xFFFFFFFFu, my_found, leader);
+  const uint64_t val = __shfl_sync(0xFFFFFFFFu, my_val, leader);
+  if (!active) return;
+  if (out_kind == kOutResult) {
+    uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
+    st_cs_u64(p, found ? 1ull : 0ull);
+    st_cs_u64(p + 1, found ? val : 0ull);
+  } else if (out_kind == kOutResult32) {
+    st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
+  } else if (out_kind == kOutBool) {
+    st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+  }
+}
+
 // Ordering of the window's big groups; when hot keys produced groups of
 // more than kSortSmall members, the grid (a cooperative launch) continues
 // with the huge_* steps between grid barriers.
@@ -721,13 +797,14 @@ struct Tuning {
   uint32_t chunk = 0;    // probe work claim (0 = static stride)
   uint32_t prefetch = 0; // extra lookups in flight per thread (0..2)
   uint32_t dedup = 0;
+  uint32_t warp_probe = 0;  // read-only batches through k_read_coop
 };
 
 inline bool tuning_ok(const lsb_tuning& x) {
   return (x.block_threads == 128 || x.block_threads == 256 || x.block_threads == 512 ||
           x.block_threads == 1024) &&
          x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
-         x.fused_split <= 100 && x.region_order <= 1;
+         x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1;
 }
 
 template <class Tr>
@@ -869,6 +946,7 @@ struct Table {
     tune.chunk = x.chunk;
     tune.prefetch = x.prefetch;
     tune.dedup = x.dedup;
+    tune.warp_probe = x.warp_probe;
     split_q16 = (uint32_t)(((uint64_t)x.fused_split << 16) / 100);
     binned = x.region_order != 0;
     return LSB_OK;
@@ -881,6 +959,7 @@ struct Table {
     x->dedup = tune.dedup;
     x->fused_split = (uint32_t)(((uint64_t)split_q16 * 100 + 32768) >> 16);
     x->region_order = binned ? 1u : 0u;
+    x->warp_probe = tune.warp_probe;
   }
 
   // Epoch of the next per-phase window (even: 2, 4, ...; the fused path uses
@@ -941,9 +1020,13 @@ struct Table {
     if (!tune.dedup && lock_mode != kLockRW) {
       for (size_t off = 0; off < n; off += (size_t)1 << 30) {
         const uint32_t m = (uint32_t)std::min<size_t>((size_t)1 << 30, n - off);
-        k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(
-            view(), keys + off, out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr,
-            out ? out_kind : kOutNone, m);
+        void* o = out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr;
+        if (tune.warp_probe)
+          k_read_coop<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), keys + off, o,
+                                                          out ? out_kind : kOutNone, m);
+        else
+          k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), keys + off, o,
+                                                     out ? out_kind : kOutNone, m);
         LSB_CK(cudaGetLastError());
       }
       return LSB_OK;
@@ -1213,32 +1296,36 @@ int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::K
   float best_ms = 1e30f;
   lsb_tuning win = cur;
   int err = LSB_OK;
-  for (uint32_t block : {256u, 512u, 1024u}) {
+  // 4, 8, 16 and 32 warps a block; lookahead 0..2; the list-first order
+  // (its reads claim whole blocks of ops; with in-warp dedup the claim size
+  // is tuned below), or one pass with the probe's claim size static or
+  // 32..4096 ops.  Each candidate: one warm-up run, then the median of three.
+  static const uint32_t kChunks[] = {0u, 32u, 128u, 512u, 1024u, 2048u, 4096u};
+  constexpr int kReps = 3;
+  for (uint32_t block : {128u, 256u, 512u, 1024u}) {
     for (uint32_t prefetch : {0u, 1u, 2u}) {
-      // split 0: chunk = the reads' claim size; split 100: the probe's
-      for (uint32_t cand = 0; cand < 9; ++cand) {
-        static const uint32_t kChunks[9] = {0u, 2048u, 4096u, 8192u, 16384u, 0u, 1024u, 2048u, 4096u};
+      for (uint32_t cand = 0; cand < 1 + sizeof(kChunks) / sizeof(kChunks[0]); ++cand) {
         lsb_tuning c = cur;
         c.block_threads = block;
         c.prefetch = prefetch;
-        c.chunk = kChunks[cand];
-        c.fused_split = cand < 5 ? 0u : 100u;
+        c.fused_split = cand == 0 ? 0u : 100u;
+        c.chunk = cand == 0 ? (cur.dedup ? 2048u : 0u) : kChunks[cand - 1];
         if (tb.set_tuning(c) != LSB_OK) continue;
         if (tb.fused_grid() <= 0) continue;  // shape cannot be co-resident
         err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);  // warm-up
         if (err) break;
-        cudaEventRecord(e0, s);
-        err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);
-        cudaEventRecord(e1, s);
-        if (err) break;
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-          err = LSB_ERR_CUDA;
-          break;
+        float t[kReps];
+        for (int r = 0; r < kReps && !err; ++r) {
+          cudaEventRecord(e0, s);
+          err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);
+          cudaEventRecord(e1, s);
+          if (!err && cudaEventSynchronize(e1) != cudaSuccess) err = LSB_ERR_CUDA;
+          if (!err) cudaEventElapsedTime(&t[r], e0, e1);
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-          best_ms = ms;
+        if (err) break;
+        std::sort(t, t + kReps);
+        if (t[kReps / 2] < best_ms) {
+          best_ms = t[kReps / 2];
           win = c;
         }
       }

@@ -338,9 +338,9 @@ def test_empty_and_bad_arguments(cuda):
     assert m.buckets() == 16
 
 
-@pytest.mark.parametrize("block", [256, 1024])
+@pytest.mark.parametrize("block", [128, 256, 1024])
 @pytest.mark.parametrize("prefetch", [0, 1, 2])
-@pytest.mark.parametrize("chunk", [0, 2048])
+@pytest.mark.parametrize("chunk", [0, 32, 2048])
 @pytest.mark.parametrize("split", [0, 100])
 @pytest.mark.parametrize("dedup", [0, 1])
 def test_every_tuning_is_exact(cuda, block, prefetch, chunk, split, dedup):
@@ -414,3 +414,29 @@ def test_lock_free_inserts_do_not_waste_slabs(cuda):
     k, v = m.dump()
     ok, ov = o.dump()
     assert np.array_equal(k, ok) and np.array_equal(v, ov)
+
+
+def test_warp_cooperative_probe_reads_exact(cuda):
+    """The warp-cooperative slab probe (tuning warp_probe=1, the reference's
+    probe structure) answers read-only batches exactly like the default
+    probe: long chains, absent keys, keys repeated inside warps, key 0."""
+    log2 = 6
+    keys = W.prefill_keys(91, 40_000)  # ~625 keys a bucket: chains of ~23 slabs
+    m = Map(log2, 1 << 13)
+    m.put(dev(keys), dev(keys ^ np.uint64(5)))
+    m.remove(dev(keys[::7]))
+    o = OracleMap(log2)
+    o.put(keys, keys ^ np.uint64(5))
+    o.remove(keys[::7])
+    rng = np.random.default_rng(91)
+    q = np.concatenate([keys[rng.integers(0, len(keys), 30_000)], W.absent_keys(92, 5000, keys),
+                        np.zeros(100, np.uint64), np.repeat(keys[:50], 20)])
+    want = o.get(q)
+    for wp in (1, 0):
+        m.set_tuning(warp_probe=wp)
+        out = results_buf(len(q))
+        m.get(dev(q), out)
+        _sync()
+        got = results(out)
+        assert same_results(got, want), f"warp_probe={wp}: " + first_mismatch(got, want)
+    assert m.status() == 0

@@ -108,3 +108,22 @@ def test_pool_not_wasted_by_concurrent_inserts(cuda):
     # Poisson(56) keys per bucket need ~1.47 overflow slabs per bucket; each
     # SM may hold one partly used chunk (at most 32 slabs) on top
     assert used <= int(1.55 * buckets) + 148 * 32, (used, buckets)
+
+
+def test_set_warp_cooperative_probe_exact(cuda):
+    keys = W.perm32(np.arange(50_000))
+    s = Set(6, 1 << 12)
+    s.insert(dev(keys))
+    s.remove(dev(keys[::3]))
+    o = OracleSet(6)
+    o.insert(keys)
+    o.remove(keys[::3])
+    q = W.perm32(np.arange(0, 100_000, 2))
+    want = o.contains(q)
+    for wp in (1, 0):
+        s.set_tuning(warp_probe=wp)
+        out = cuda.zeros(len(q), dtype=cuda.uint8, device="cuda")
+        s.contains(dev(q), out)
+        cuda.cuda.synchronize()
+        assert np.array_equal(host(out, np.uint8), want), f"warp_probe={wp}"
+    assert s.status() == 0
