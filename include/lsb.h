@@ -425,6 +425,45 @@ typedef struct lsb_serve_load {
 int lsb_serve_run_load(lsb_server* s, const lsb_serve_load* load, uint64_t* latency_ns,
                        uint64_t* wall_ns);
 
+/* ---- KV store: variable-size byte values --------------------------------
+ * A caller layer over the map (no counterpart in the reference library; its
+ * KVCG tests keep value pointers in the map, test/slabunified_test.cu:
+ * 360-380): values live in one device byte heap of heap_bytes (at most 2^40),
+ * the map holds key -> heap offset and length (values up to 2^24 - 1 bytes).
+ * All arrays are device memory; calls are stream-ordered like the map's. */
+typedef struct lsb_kvs lsb_kvs;
+int lsb_kvs_create(unsigned log2_buckets, uint64_t heap_bytes, const lsb_options* opt,
+                   lsb_kvs** out);
+int lsb_kvs_destroy(lsb_kvs* s);
+/* The map underneath (for lsb_map_size, _status, _compact...). */
+lsb_map* lsb_kvs_map(lsb_kvs* s);
+/* Put n values: op i's bytes are vals[val_off[i] .. val_off[i+1]) (n + 1
+ * offsets, non-decreasing).  Ops run in index order; the space of a replaced
+ * value becomes garbage (lsb_kvs_usage) until lsb_kvs_compact.  LSB_ERR_OOM
+ * (no effect) when the heap cannot take the batch; LSB_ERR_ARG when a value
+ * is too long.  Synchronises the stream (the batch's size is read). */
+int lsb_kvs_put(lsb_kvs* s, const uint64_t* keys, const uint8_t* vals, const uint64_t* val_off,
+                size_t n, cudaStream_t stream);
+/* Get n values: found_out[i] (optional) = the key is present, len_out[i] =
+ * the value's length (0 when absent), dst_off_out[i] = its offset in dst (the
+ * exclusive prefix sums of the lengths), and the bytes copied to dst when it
+ * is not NULL (values that would end past dst_cap are not copied).
+ * *total_out (optional; synchronises) receives the bytes all found values
+ * need. */
+int lsb_kvs_get(lsb_kvs* s, const uint64_t* keys, uint8_t* found_out, uint32_t* len_out,
+                uint64_t* dst_off_out, uint8_t* dst, uint64_t dst_cap, size_t n,
+                uint64_t* total_out, cudaStream_t stream);
+/* Remove n keys; found_out[i] (optional) = the key was present. */
+int lsb_kvs_remove(lsb_kvs* s, const uint64_t* keys, uint8_t* found_out, size_t n,
+                   cudaStream_t stream);
+/* Heap bytes handed out, bytes of replaced or removed values among them, and
+ * the capacity (synchronises). */
+int lsb_kvs_usage(lsb_kvs* s, uint64_t* heap_used, uint64_t* heap_dead, uint64_t* heap_cap,
+                  cudaStream_t stream);
+/* Move the live values to the front of the heap (key order) and drop the
+ * garbage; must not overlap other calls on the store.  Synchronises. */
+int lsb_kvs_compact(lsb_kvs* s, cudaStream_t stream);
+
 /* ---- device per-warp API -------------------------------------------------
  * The device methods of the reference (map::get/put/update, map.h:92-183;
  * set::contains/insert/remove, set.h:64-90) are in include/lsb_device.cuh,

@@ -27,7 +27,7 @@ from ._lib import (LOCK_FREE, LOCK_RW, LOCK_WRITER, OP_CONTAINS, OP_GET, OP_INSE
                    LsbError)
 
 __all__ = [
-    "Map", "Set", "Server", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_UPDATE", "OP_CONTAINS",
+    "Map", "Set", "Server", "KVStore", "LsbError", "OP_GET", "OP_PUT", "OP_REMOVE", "OP_UPDATE", "OP_CONTAINS",
     "OP_INSERT",
     "LOCK_WRITER", "LOCK_FREE", "LOCK_RW", "STATUS_OOM", "STATUS_TIMEOUT", "STATUS_CHAIN",
     "STATUS_BARRIER", "STATUS_SCRATCH", "lib",
@@ -398,3 +398,64 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class KVStore:
+    """Variable-size byte values keyed by uint64 (lsb_kvs_*, include/lsb.h):
+    values in a device heap of heap_bytes, the map holding key -> (offset,
+    length).  put/get/remove take device tensors; get_values is a host-side
+    convenience returning Python bytes."""
+
+    def __init__(self, n_log_2: int, heap_bytes: int, pool_slabs: int = 0, *,
+                 max_window: int = 0, lock_mode="writer", device: int = -1):
+        self._h = None
+        h = C.c_void_p()
+        _lib.check(lib().lsb_kvs_create(int(n_log_2), int(heap_bytes),
+                                        C.byref(_opts(pool_slabs, max_window, lock_mode, device)),
+                                        C.byref(h)), "lsb_kvs_create")
+        self._h = h
+
+    def _call(self, name, *args):
+        _lib.check(getattr(lib(), f"lsb_kvs_{name}")(self._h, *args), f"lsb_kvs_{name}")
+
+    def close(self):
+        if self._h is not None:
+            lib().lsb_kvs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def put(self, keys, vals, val_off, size=None, stream=None):
+        """vals: uint8 device buffer of the packed values; val_off: n + 1
+        int64 offsets into it."""
+        self._call("put", _ptr(keys), _ptr(vals), _ptr(val_off), _len(keys, size), _stream(stream))
+
+    def get(self, keys, len_out, dst_off_out, dst=None, dst_cap=0, found_out=None, size=None,
+            stream=None) -> int:
+        """Found flags, lengths and destination offsets (and the bytes, into
+        dst); returns the bytes all found values need."""
+        total = C.c_uint64()
+        self._call("get", _ptr(keys), _ptr(found_out), _ptr(len_out), _ptr(dst_off_out), _ptr(dst),
+                   int(dst_cap), _len(keys, size), C.byref(total), _stream(stream))
+        return int(total.value)
+
+    def remove(self, keys, found_out=None, size=None, stream=None):
+        self._call("remove", _ptr(keys), _ptr(found_out), _len(keys, size), _stream(stream))
+
+    def usage(self, stream=None) -> dict:
+        u, d, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self._call("usage", C.byref(u), C.byref(d), C.byref(c), _stream(stream))
+        return {"heap_used": int(u.value), "heap_dead": int(d.value), "heap_cap": int(c.value)}
+
+    def compact(self, stream=None):
+        self._call("compact", _stream(stream))
+
+    def size(self, stream=None) -> int:
+        v = C.c_uint64()
+        _lib.check(lib().lsb_map_size(lib().lsb_kvs_map(self._h), C.byref(v), _stream(stream)),
+                   "lsb_map_size")
+        return int(v.value)

@@ -118,6 +118,14 @@ _SIGS = {
     "lsb_map_put_pairs": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_update": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_kvs_create": (C.c_int, [C.c_uint, C.c_uint64, _P, _P]),
+    "lsb_kvs_destroy": (C.c_int, [_P]),
+    "lsb_kvs_map": (_P, [_P]),
+    "lsb_kvs_put": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
+    "lsb_kvs_get": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_uint64, _SZ, _P, _P]),
+    "lsb_kvs_remove": (C.c_int, [_P, _P, _P, _SZ, _P]),
+    "lsb_kvs_usage": (C.c_int, [_P, _P, _P, _P, _P]),
+    "lsb_kvs_compact": (C.c_int, [_P, _P]),
     "lsb_map_device_view": (C.c_int, [_P, _P]),
     "lsb_set_device_view": (C.c_int, [_P, _P]),
     "lsb_map_get_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
