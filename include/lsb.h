@@ -123,7 +123,8 @@ typedef struct lsb_tuning {
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */
-#define LSB_LOCK_FREE 1u     /* writers claim slots with CAS on slab words, no lock   */
+#define LSB_LOCK_FREE 1u     /* writers claim slots with CAS on slab words; growing a
+                                full chain takes the bucket lock */
 #define LSB_LOCK_RW 2u       /* reference-style: readers take a shared bucket lock too */
 
 /* ---- map<uint64_t, uint64_t> ------------------------------------------

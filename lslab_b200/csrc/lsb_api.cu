@@ -56,6 +56,9 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_FUSED_LEAN_READS
 #define LSB_FUSED_LEAN_READS 1
 #endif
+#ifndef LSB_FUSED_READ_PAIR
+#define LSB_FUSED_READ_PAIR 1
+#endif
 template <class Tr, bool kGroup, int P>
 __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
@@ -301,8 +304,8 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
         phase_bin_scatter<Tr>(w, sc.obin, sc.perm, &job.bins[wi & 1]);
         perm = sc.perm;
       } else if (lean_reads) {
-        phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, w.n, &w.cnt->tiles_done,
-                            (listed + 31) / 32);
+        phase_read_lean<Tr, LSB_FUSED_READ_PAIR != 0>(t, w, &w.cnt->late_cursor, 0, w.n,
+                                                      &w.cnt->tiles_done, (listed + 31) / 32);
       } else {
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor, late_chunk,
                                   job.dedup != 0, ProbeSel{0, w.n, false}, 0, nullptr,
@@ -332,7 +335,7 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
       if (has_big) phase_sort_big<Tr>(sc, w, smem);
       if (has_huge) huge_hist<Tr>(sc, w, warp, nwarps);
       if (split < w.n && lean_reads && split == 0 && perm == nullptr)
-        phase_read_lean<Tr>(t, w, &w.cnt->late_cursor, 0, w.n);
+        phase_read_lean<Tr, LSB_FUSED_READ_PAIR != 0>(t, w, &w.cnt->late_cursor, 0, w.n);
       else if (split < w.n)  // claimed, so blocks freed by the sort take more
         phase_probe<Tr, false, P>(t, sc, w, warp, nwarps, &w.cnt->late_cursor,
                                   late_chunk, job.dedup != 0, ProbeSel{split, w.n, false},
@@ -352,7 +355,7 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     // window's resolve and takes no resolve work
     const uint32_t r0 = Hook::kActive ? 32u : 0u;
     if (Hook::kActive && wi + 1 == nwin && tid < 32) hook();
-    if (has_mut && tid >= r0) {
+    if (has_mut && (!Hook::kActive || tid >= r0)) {
       // Mutations and the reads after the first mutation resolve
       // independently.  A small window (every thread holds at most one item
       // of each kind) runs them side by side on two shares of the grid, so

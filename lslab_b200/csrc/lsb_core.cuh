@@ -690,36 +690,20 @@ __device__ void table_apply_locked(const TableView& t, typename Tr::Key key, uin
   unlock_writer(t, bucket);
 }
 
-// Append an empty slab (ours, unlinked) at the end of bucket's chain, where
-// later inserts into the bucket find its slots.  Lock-free: CAS on the tail's
-// link, following the chain when another slab got there first.
-__device__ __noinline__ inline void link_spare(const TableView& t, uint32_t bucket, uint32_t spare,
-                                               uint32_t slab_bytes) {
-  uint32_t s = bucket;
-  for (uint32_t hop = 0; hop < kMaxHops; ++hop) {
-    uint32_t* link = (uint32_t*)slab_ptr(t.slabs, s, slab_bytes);
-    const uint32_t next = atomicCAS(link, 0u, spare);
-    if (next == 0u) return;
-    s = next;
-  }
-  raise_status(t.status, kStatusChain);
-}
-
 template <class Tr>
 __device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, uint64_t h,
                                      bool present, uint64_t val) {
   const uint32_t bucket = (uint32_t)h & t.mask;
   const uint32_t fp = fingerprint(h);
-  // A full chain grows by an EMPTY slab linked at the tail by CAS; the insert
-  // then claims a slot by CAS like any other.  A thread that loses the link
-  // race keeps its slab (pool slabs are zeroed) for a later attempt, and one
-  // still unused when the op is done is appended to the chain, so racing
-  // inserts waste no slab; an empty slab left in a chain is taken by later
-  // inserts into the bucket, or returned by compaction.
-  uint32_t spare = 0;
+  // Slots are claimed with CAS on the tag words (no lock).  Growing a full
+  // chain is serialized on the bucket's lock word: the holder re-reads the
+  // tail's link and, if it is still empty, links one zeroed slab; every other
+  // insert that found the chain full rescans from the tail once the lock is
+  // released.  (Linking without it, each racer would link or drop a slab of
+  // its own: hundreds of concurrent inserts into one bucket exhausted the
+  // pool that way.)
   uint32_t start = bucket;
-  bool done = false;
-  for (uint32_t attempt = 0; attempt < kLockPolls && !done; ++attempt) {
+  for (uint32_t attempt = 0; attempt < kLockPolls; ++attempt) {
     ScanResult r;
     r.found_slot = -1;
     r.free_slot = -1;
@@ -757,13 +741,9 @@ __device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, u
       } else if (r.found_live) {
         atomicAnd(tw, ~(0x80u << sh));
       }
-      done = true;
-      break;
+      return;
     }
-    if (!present) {
-      done = true;
-      break;
-    }
+    if (!present) return;
     if (r.free_slot >= 0) {
       uint8_t* slab = slab_ptr(t.slabs, r.free_slab, Tr::kSlabBytes);
       uint32_t* tw = tag_word(slab, r.free_slot);
@@ -777,25 +757,30 @@ __device__ void table_apply_lockfree(const TableView& t, typename Tr::Key key, u
           key_store<Tr>(slab + kMetaBytes + r.free_slot * Tr::kSlotBytes, key, val);
           __threadfence();
           atomicXor(tw, (0x80u ^ (0x80u | fp)) << sh);  // busy -> live
-          done = true;
-          break;
+          return;
         }
       }
       start = bucket;  // lost the race: rescan from the head
       continue;
     }
-    // the chain is full: link an empty slab at its tail, then rescan from the
-    // old tail (its successor now exists, ours or a racer's)
-    if (spare == 0) {
-      spare = pool_alloc(t);
-      if (spare == 0) return;  // OOM raised
-    }
+    // the chain is full: grow it by one slab under the bucket's lock word
+    if (!lock_writer(t, bucket)) return;  // timeout raised
     uint32_t* link = (uint32_t*)slab_ptr(t.slabs, r.tail, Tr::kSlabBytes);
-    if (atomicCAS(link, 0u, spare) == 0u) spare = 0;
-    start = r.tail;
+    bool oom = false;
+    if (ld_cg_u32(link) == 0) {
+      const uint32_t n = pool_alloc(t);  // zeroed: every slot empty
+      if (n != 0) {
+        __threadfence();
+        atomicExch(link, n);
+      } else {
+        oom = true;  // raised by pool_alloc
+      }
+    }
+    unlock_writer(t, bucket);
+    if (oom) return;
+    start = r.tail;  // rescan from the old tail: its successor now exists
   }
-  if (!done) raise_status(t.status, kStatusTimeout);
-  if (spare != 0) link_spare(t, bucket, spare, Tr::kSlabBytes);
+  raise_status(t.status, kStatusTimeout);
 }
 
 template <class Tr>

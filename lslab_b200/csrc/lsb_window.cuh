@@ -587,7 +587,10 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
 // With stop_at, a block takes no further claim once *stop_at has reached
 // stop_target (the rest is claimed by a later call on the same cursor).
 // Every thread of the block calls it.
-template <class Tr>
+// kPair: each thread keeps two lookups in flight (both meta sectors, then
+// both candidate slots; table_find_n), which recovers the memory
+// parallelism that a 64-register kernel's half occupancy loses.
+template <class Tr, bool kPair = false>
 __device__ void phase_read_lean(const TableView& t, const Window<Tr>& w, uint32_t* cursor,
                                 uint32_t lo, uint32_t hi, const uint32_t* stop_at = nullptr,
                                 uint32_t stop_target = 0) {
@@ -603,11 +606,29 @@ __device__ void phase_read_lean(const TableView& t, const Window<Tr>& w, uint32_
     __syncthreads();  // s_base is rewritten next round
     if (c0 >= hi || c0 < lo) break;  // block-uniform
     const uint32_t c1 = min(hi, c0 + chunk);
-    for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-      if (op_type(w, i) != kOpRead) continue;
-      uint64_t val;
-      const bool found = read_lookup<Tr>(t, key_stream(w, i), &val);
-      write_result(w, i, kOpRead, found, val);
+    if constexpr (kPair) {
+      for (uint32_t i = c0 + threadIdx.x; i < c1; i += 2 * blockDim.x) {
+        const uint32_t i2 = i + blockDim.x;
+        typename Tr::Key key[2];
+        uint64_t h[2], val[2], loc[2];
+        bool want[2], found[2];
+        want[0] = op_type(w, i) == kOpRead;
+        want[1] = i2 < c1 && op_type(w, i2) == kOpRead;
+        key[0] = want[0] ? key_stream(w, i) : (typename Tr::Key)0;
+        key[1] = want[1] ? key_stream(w, i2) : (typename Tr::Key)0;
+        h[0] = Tr::hash(key[0]);
+        h[1] = Tr::hash(key[1]);
+        table_find_n<Tr, 2>(t, key, h, want, found, val, loc);
+        if (want[0]) write_result(w, i, kOpRead, found[0], val[0]);
+        if (want[1]) write_result(w, i2, kOpRead, found[1], val[1]);
+      }
+    } else {
+      for (uint32_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+        if (op_type(w, i) != kOpRead) continue;
+        uint64_t val;
+        const bool found = read_lookup<Tr>(t, key_stream(w, i), &val);
+        write_result(w, i, kOpRead, found, val);
+      }
     }
   }
 }

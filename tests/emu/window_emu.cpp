@@ -42,6 +42,9 @@ int main(int argc, char** argv) {
   const bool muts_first = binned || (argc == 7 && std::strcmp(argv[6], "muts_first") == 0);
   const bool compact = argc == 7 && std::strcmp(argv[6], "compact") == 0;
   const bool lockfree = argc == 7 && std::strcmp(argv[6], "lockfree") == 0;
+  // mode v32put: every op a put (types ignored), 32-bit values (the low half
+  // of each value), 32-bit old values out (lsb_map_put_v32's window)
+  const bool v32put = argc == 7 && std::strcmp(argv[6], "v32put") == 0;
   FILE* f = std::fopen(argv[1], "rb");
   if (!f) return 2;
   uint32_t n = 0, window = 0;
@@ -79,6 +82,8 @@ int main(int argc, char** argv) {
   Scratch sc;
   emu::alloc_scratch(sc, window, t.status, keep);
   uint8_t* out = (uint8_t*)alloc(16ull * n);
+  uint32_t* vals32 = (uint32_t*)alloc(4ull * n);
+  for (uint32_t i = 0; i < n; ++i) vals32[i] = (uint32_t)vals[i];
   std::vector<uint32_t> smem(kSortSmemBytes / 4);
   BinCounters* bins = (BinCounters*)alloc(sizeof(BinCounters));
   const uint32_t bin_shift = log2 > kBinBits ? log2 - kBinBits : 0u;
@@ -97,6 +102,14 @@ int main(int argc, char** argv) {
     epoch += 2;
     w.epoch = epoch;
     w.out_kind = kOutResult;
+    if (v32put) {
+      w.types = nullptr;
+      w.uniform = kOpWrite;
+      w.vals = reinterpret_cast<const uint64_t*>(vals32 + off);
+      w.v32 = 1;
+      w.out = out + (size_t)off * 4;
+      w.out_kind = kOutOld32;
+    }
     w.cnt = &sc.cnt[0];
     std::memset(sc.cnt, 0, 2 * sizeof(WinCounters));
     std::memset(bins, 0, sizeof(BinCounters));
@@ -159,7 +172,7 @@ int main(int argc, char** argv) {
   }
   FILE* o = std::fopen(argv[5], "wb");
   if (!o) return 2;
-  std::fwrite(out, 16, n, o);
+  std::fwrite(out, v32put ? 4 : 16, n, o);
   std::fwrite(t.status, 4, 1, o);
   std::fwrite(&t.pool[0], 8, 1, o);
   std::fwrite(&t.pool[kPoolTop], 8, 1, o);

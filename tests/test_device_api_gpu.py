@@ -88,7 +88,8 @@ def test_one_warp_is_sequential(cuda, lib, lock_mode):
     t, k, v = _map_batch(3, 6000, 300)
     m = Map(6, lock_mode=lock_mode)
     out = results_buf(len(k))
-    assert lib.dev_map_ops(m.handle, dev(t).data_ptr(), dev(k).data_ptr(), dev(v).data_ptr(),
+    dt, dk, dv = dev(t), dev(k), dev(v)  # held until the kernel has run
+    assert lib.dev_map_ops(m.handle, dt.data_ptr(), dk.data_ptr(), dv.data_ptr(),
                            out.data_ptr(), len(k), 1, None) == 0
     _sync()
     want = _want_map(OracleMap(6), t, k, v)
@@ -115,7 +116,8 @@ def test_many_warps_on_disjoint_keys(cuda, lib):
     t, k, v = _method_order(t, k, v)
     m = Map(10, 1 << 14)
     out = results_buf(n)
-    assert lib.dev_map_ops(m.handle, dev(t).data_ptr(), dev(k).data_ptr(), dev(v).data_ptr(),
+    dt, dk, dv = dev(t), dev(k), dev(v)
+    assert lib.dev_map_ops(m.handle, dt.data_ptr(), dk.data_ptr(), dv.data_ptr(),
                            out.data_ptr(), n, 0, None) == 0
     _sync()
     want = _want_map(OracleMap(10), t, k, v)
@@ -137,7 +139,8 @@ def test_many_warps_on_hot_keys_stay_consistent(cuda, lib):
     v = np.arange(1, n + 1, dtype=np.uint64)  # each put writes a distinct value
     m = Map(4)
     out = results_buf(n)
-    assert lib.dev_map_ops(m.handle, dev(t).data_ptr(), dev(k).data_ptr(), dev(v).data_ptr(),
+    dt, dk, dv = dev(t), dev(k), dev(v)
+    assert lib.dev_map_ops(m.handle, dt.data_ptr(), dk.data_ptr(), dv.data_ptr(),
                            out.data_ptr(), n, 0, None) == 0
     _sync()
     got = results(out)
@@ -169,7 +172,8 @@ def test_set_device_api_one_warp(cuda, lib):
     t, k = t[o], k[o]
     s = Set(5)
     out = cuda.zeros(n, dtype=cuda.uint8, device="cuda")
-    assert lib.dev_set_ops(s.handle, dev(t).data_ptr(), dev(k).data_ptr(), out.data_ptr(),
+    dt, dk = dev(t), dev(k)
+    assert lib.dev_set_ops(s.handle, dt.data_ptr(), dk.data_ptr(), out.data_ptr(),
                            n, 1, None) == 0
     _sync()
     o = OracleSet(5)

@@ -249,3 +249,26 @@ def test_lock_free_inserts_race_without_losing_keys_or_slabs(bins, tmp_path):
     assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}"
     needed = n // 28 - (1 << log2)  # overflow slabs of perfectly packed chains
     assert cursor - (1 << log2) <= needed + 2 * (1 << log2) + 64, (cursor, needed)
+
+
+def test_v32_put_batch_equals_oracle(bins, tmp_path):
+    """A put batch with 32-bit values and 32-bit old values out (the window
+    lsb_map_put_v32 runs), keys repeated across the batch: every old value
+    equals the oracle's."""
+    rng = np.random.default_rng(32)
+    n, log2 = 12_000, 6
+    k = W.key_of_rank(32, rng.integers(0, 4000, size=n).astype(np.uint64))
+    v = rng.integers(0, 2**32, size=n, dtype=np.uint64)
+    path, outp = tmp_path / "ops.bin", tmp_path / "out.bin"
+    _write_window(path, np.ones(n, np.uint8), k, 16_384, v)
+    want = OracleMap(log2).put(k, v)
+    pool = (1 << log2) // 4 + 4096
+    r = subprocess.run([str(bins["window"]), str(path), str(log2), str(pool), "256", str(outp),
+                        "v32put"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout + r.stderr[-4000:]
+    raw = np.fromfile(outp, np.uint8)
+    got = raw[: 4 * n].view(np.uint32)
+    status = int(raw[4 * n:4 * n + 4].view(np.uint32)[0])
+    assert status == 0
+    bad = np.nonzero(got != want.astype(np.uint32))[0]
+    assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}: {got[bad[:3]]} vs {want[bad[:3]]}"

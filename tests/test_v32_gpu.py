@@ -42,8 +42,10 @@ def test_v32_put_get_update_equal_the_oracle(cuda):
     o = OracleMap(log2)
     # SoA put (repeated keys: old values chain in index order)
     old = cuda.zeros(n * 4, dtype=cuda.uint8, device="cuda")
-    _call("lsb_map_put_v32", m.handle, _dev(keys).data_ptr(), _dev(vals).data_ptr(),
-          old.data_ptr(), n, None)
+    # device copies held in variables until the calls are done (a temporary's
+    # memory could be reused by the next allocation before the kernel runs)
+    dk, dv = _dev(keys), _dev(vals)
+    _call("lsb_map_put_v32", m.handle, dk.data_ptr(), dv.data_ptr(), old.data_ptr(), n, None)
     want_old = o.put(keys, vals.astype(np.uint64))
     cuda.cuda.synchronize()
     assert np.array_equal(_host(old, np.uint32), want_old.astype(np.uint32))
@@ -53,7 +55,8 @@ def test_v32_put_get_update_equal_the_oracle(cuda):
     pairs = np.zeros(n, KV32)
     pairs["key"], pairs["value"] = pk, pv
     old2 = cuda.zeros(n * 4, dtype=cuda.uint8, device="cuda")
-    _call("lsb_map_put_pairs_v32", m.handle, _dev(pairs).data_ptr(), old2.data_ptr(), n, None)
+    dp = _dev(pairs)
+    _call("lsb_map_put_pairs_v32", m.handle, dp.data_ptr(), old2.data_ptr(), n, None)
     want_old2 = o.put(pk, pv.astype(np.uint64))
     cuda.cuda.synchronize()
     assert np.array_equal(_host(old2, np.uint32), want_old2.astype(np.uint32))
@@ -63,7 +66,8 @@ def test_v32_put_get_update_equal_the_oracle(cuda):
     up = np.zeros(len(uk), KV32)
     up["key"], up["value"] = uk, uv
     uout = cuda.zeros(len(uk) * 8, dtype=cuda.uint8, device="cuda")
-    _call("lsb_map_update_v32", m.handle, _dev(up).data_ptr(), uout.data_ptr(), len(uk), None)
+    du = _dev(up)
+    _call("lsb_map_update_v32", m.handle, du.data_ptr(), uout.data_ptr(), len(uk), None)
     want_u = o.update(uk, uv.astype(np.uint64))
     cuda.cuda.synchronize()
     gu = _host(uout, R32)
@@ -72,7 +76,8 @@ def test_v32_put_get_update_equal_the_oracle(cuda):
     # get, present and absent
     q = np.concatenate([keys[:10000], uk])
     gout = cuda.zeros(len(q) * 8, dtype=cuda.uint8, device="cuda")
-    _call("lsb_map_get_v32", m.handle, _dev(q).data_ptr(), gout.data_ptr(), len(q), None)
+    dq = _dev(q)
+    _call("lsb_map_get_v32", m.handle, dq.data_ptr(), gout.data_ptr(), len(q), None)
     want_g = o.get(q)
     cuda.cuda.synchronize()
     g = _host(gout, R32)
