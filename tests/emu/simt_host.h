@@ -1,7 +1,7 @@
 // Host emulation of the CUDA execution model, for CPU tests of the library's
 // device functions (test infrastructure; never linked into the library).
 //
-// Every thread of an emulated block is a std::thread.  __syncthreads is a
+// Every thread of an emulated block is a host thread (of a reused pool).  __syncthreads is a
 // barrier over the block; a warp intrinsic is an exchange through a per-warp
 // buffer between two barriers over the warp's 32 threads, so every lane must
 // take part (the library only uses full-warp masks).  Shared-memory variables
@@ -13,8 +13,11 @@
 #include <barrier>
 #include <cassert>
 #include <cstdint>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -68,6 +71,72 @@ inline T from64(uint64_t r) {
   return v;
 }
 
+// A pool of host threads, created once and reused for every block (creating
+// a block's threads afresh per block dominated the run time under
+// AddressSanitizer).  Worker t runs the posted block's f() as threadIdx.x = t.
+class Pool {
+ public:
+  static Pool& get() {
+    static Pool p;
+    return p;
+  }
+  void run(unsigned nthreads, unsigned block, Block* b, const std::function<void()>& f) {
+    std::unique_lock<std::mutex> lk(mu_);
+    while (workers_.size() < nthreads) {
+      const unsigned t = (unsigned)workers_.size();
+      // gen_ is still the previous block's: the new worker takes this block
+      workers_.emplace_back([this, t, g = gen_] { loop(t, g); });
+    }
+    job_ = &f;
+    blk_ = b;
+    block_ = block;
+    active_ = nthreads;
+    left_ = nthreads;
+    ++gen_;
+    start_.notify_all();
+    done_.wait(lk, [this] { return left_ == 0; });
+    job_ = nullptr;
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      ++gen_;
+    }
+    start_.notify_all();
+    for (auto& w : workers_) w.join();
+  }
+
+ private:
+  void loop(unsigned t, uint64_t seen) {
+    for (;;) {
+      const std::function<void()>* f;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        start_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (stop_) return;
+        if (t >= active_) continue;
+        f = job_;
+        threadIdx.x = t;
+        blockIdx.x = block_;
+        blk = blk_;
+      }
+      (*f)();
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--left_ == 0) done_.notify_one();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable start_, done_;
+  std::vector<std::thread> workers_;
+  const std::function<void()>* job_ = nullptr;
+  Block* blk_ = nullptr;
+  unsigned block_ = 0, active_ = 0, left_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
 // Runs f() on every thread of one block of `nthreads` (a multiple of 32).
 template <class F>
 void run_block(unsigned nthreads, unsigned block, unsigned nblocks, F&& f) {
@@ -79,16 +148,8 @@ void run_block(unsigned nthreads, unsigned block, unsigned nblocks, F&& f) {
   b.buf.assign(nthreads, 0);
   blockDim.x = nthreads;
   gridDim.x = nblocks;
-  std::vector<std::thread> th;
-  th.reserve(nthreads);
-  for (unsigned t = 0; t < nthreads; ++t)
-    th.emplace_back([&, t] {
-      threadIdx.x = t;
-      blockIdx.x = block;
-      blk = &b;
-      f();
-    });
-  for (auto& x : th) x.join();
+  const std::function<void()> job = [&] { f(); };
+  Pool::get().run(nthreads, block, &b, job);
 }
 
 }  // namespace emu
