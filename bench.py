@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--dedup", type=int, default=-1)
     ap.add_argument("--split", type=int, default=-1, help="fused: percent of reads probed first")
     ap.add_argument("--region", type=int, default=-1, help="fused: probe in table-region order")
+    ap.add_argument("--overlap", type=int, default=-1,
+                    help="batched calls: 1 = reads in the lean read kernel beside the mutation "
+                         "steps on a second stream")
     ap.add_argument("--trace", action="store_true", help="single mode: print fused phase times")
     ap.add_argument("--single", action="store_true",
                     help="fused timing only (one table, no plain/e2e/cpu legs): the small "
@@ -234,6 +237,8 @@ def apply_tuning(args, table):
         kw["fused_split"] = args.split
     if args.region >= 0:
         kw["region_order"] = args.region
+    if args.overlap >= 0:
+        kw["overlap"] = args.overlap
     if kw:
         table.set_tuning(**kw)
 
@@ -316,7 +321,7 @@ def run_ours(args, world, rank, local):
     # the batch's net effect is one application, so the plain table applies
     # it once too and the two tables stay identical)
     explicit = (args.block or args.prefetch >= 0 or args.chunk >= 0 or args.dedup >= 0
-                or args.split >= 0 or args.region >= 0)
+                or args.split >= 0 or args.region >= 0 or args.overlap >= 0)
     if not args.no_autotune and not explicit:
         fused.autotune(d_types[0], d_keys[0], d_vals[0], out_f[0])
         g = n_get[0]
@@ -458,6 +463,34 @@ def run_ours(args, world, rank, local):
     barrier(world)
     e2e_ms = max_over_ranks(ee0.elapsed_time(ee1), world)
 
+    # the same pipeline without the table call (each step's results buffer
+    # goes back as it is): the rate the host link alone allows
+    def copy_step(b):
+        r = b % RING
+        with torch.cuda.stream(up):
+            up.wait_event(ev_out[r])
+            s_types[r].copy_(h_types[b], non_blocking=True)
+            s_keys[r].copy_(h_keys[b], non_blocking=True)
+            s_vals[r].copy_(h_vals[b], non_blocking=True)
+            ev_in[r].record(up)
+        with torch.cuda.stream(down):
+            down.wait_event(ev_in[r])
+            h_outs[r].copy_(s_out[r], non_blocking=True)
+            ev_out[r].record(down)
+
+    for b in range(args.warmup):
+        copy_step(b)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ee0.record(up)
+    for s in range(args.steps):
+        copy_step(args.warmup + s)
+    ee1.record(down)
+    torch.cuda.synchronize()
+    barrier(world)
+    copy_ms = max_over_ranks(ee0.elapsed_time(ee1), world)
+
     clk = clocks.stop()
     st |= fused.status()
 
@@ -468,9 +501,29 @@ def run_ours(args, world, rank, local):
     plain_value = ops_total / (plain_ms * 1e-3) / 1e6
     e2e_value = ops_total / (e2e_ms * 1e-3) / 1e6
     ab = [alg_bytes(batches[args.warmup + s]) for s in range(args.steps)]
-    achieved = sum(ab) / (queue_ms * 1e-3) / 1e9  # the one timed launch
+    achieved = sum(ab) / (queue_ms * 1e-3) / 1e9  # the timed call
     peak, peak_kind = peaks()
-    traffic = profiled_traffic("fused_map_cfg2")
+    tuning = fused.tuning()
+    overlap = tuning.get("overlap", 0) == 1
+    # per-window DRAM bytes of the timed form, from the committed ncu summary
+    # of a one-batch capture (not measured in this run)
+    traffic_src = "overlap_window_cfg2" if overlap else "fused_map_cfg2"
+    traffic = profiled_traffic(traffic_src)
+    windows = args.steps * ((n + (1 << 20) - 1) >> 20)  # default window: 2^20 ops
+    if overlap:
+        form = ("batched call (execute_fused) over the queue of timed batches, one 2^20-op "
+                "window per batch: its reads in the lean read kernel on the caller's stream "
+                "while its puts are listed, probed, grouped and ordered on a second, "
+                "higher-priority stream, then one resolve launch (value); the same call one "
+                "batch at a time (per_batch_launch_value); per-op-type calls: a get call and "
+                "a put call per batch (plain_value)")
+        launches = 5 * windows
+    else:
+        form = ("fused persistent kernel draining the queue of timed batches in one "
+                "launch (value); the same kernel one launch per batch "
+                "(per_batch_launch_value); per-op-type launches: a get call and a put "
+                "call per batch (plain_value)")
+        launches = 1
 
     line = {
         "metric": METRIC,
@@ -493,12 +546,9 @@ def run_ours(args, world, rank, local):
             "buckets_log2": args.buckets_log2,
             "prefill_log2": args.prefill_log2,
             "batch_ops": n,
-            "form": ("fused persistent kernel draining the queue of timed batches in one "
-                     "launch (value); the same kernel one launch per batch "
-                     "(per_batch_launch_value); per-op-type launches: a get call and a put "
-                     "call per batch (plain_value)"),
+            "form": form,
             "lock_mode": args.lock_mode,
-            "tuning": fused.tuning(),
+            "tuning": tuning,
             "l2": ("no flush: table 2^%d x 480 B = %.1f GB > L2; each step a distinct batch"
                    % (args.buckets_log2, (1 << args.buckets_log2) * 480 / 1e9)),
             "parallelism": f"{world} independent table shard(s), one per GPU",
@@ -512,12 +562,19 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": round(e2e_value, 2), "unit": "Mops/s",
                 "h2d_bytes_per_step": int(n * 17), "d2h_bytes_per_step": int(n * 16),
                 "wall_s": round(wall_e2e, 4),
-                "pipeline": "H2D, fused launch and D2H of consecutive batches on three "
-                            "streams, three buffer sets"},
-        "gpu_launches": 1,
+                "pipeline": "H2D, the batched call and D2H of consecutive batches on three "
+                            "streams, three buffer sets",
+                "copy_only_value": round(ops_total / (copy_ms * 1e-3) / 1e6, 2),
+                "copy_only": "the same pipeline and bytes without the table call",
+                "frac_of_copy_only": round(copy_ms / e2e_ms, 3)},
+        "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
+                     "traffic": traffic,
+                     "traffic_source": (f"profiles/{traffic_src}.txt: ncu DRAM bytes of one "
+                                        "2^20-op batch of this workload (committed capture, "
+                                        "not this run)"),
+                     "peak_kind": f"{peak_kind} copy bandwidth",
                      "alg_bytes_per_op": round(statistics.mean(ab) / n, 2)},
         "clocks": clk,
     }
@@ -965,57 +1022,88 @@ def _perm32(torch, idx):
 
 def run_sets(args, world, rank, local):
     """Set load-factor sweep: set<u32> with 2^18 buckets (42 MB of head slabs,
-    L2-resident) and 2^22 buckets (671 MB of heads plus the chains the load
+    L2-resident) and 2^24 buckets (2.7 GB of heads plus the chains the load
     needs, HBM-resident), prefilled to 0.25 .. 4 keys per head-slab slot;
     batches of 2^18 ops, 40% insert / 50% contains / 10% remove over a
     universe of the prefill keys and as many absent keys (uniform).  Fused:
     one execute_fused per batch; plain: per batch the insert, contains and
-    remove calls of its type-sorted parts."""
+    remove calls of its type-sorted parts; lslab: the same calls through the
+    reference's own kernels.  Checks: fused and plain give identical results
+    for every batch; lslab's contains results equal ours, its removes report
+    as many hits, and after the run a sample of 2^20 universe keys is
+    contained in lslab's table exactly where it is in ours."""
     import torch
     import lslab_b200 as L
+    import oracle
+    from oracle import RefSet
     from lslab_b200.shard import rank_seed
 
     seed = rank_seed(args.seed, rank)
     gen = torch.Generator(device="cuda")
-    gen.manual_seed(seed)
     n = 1 << 18
+    nb = args.warmup + args.steps
+    have_ref = oracle.ref_available()
     points = []
-    for log2 in (18, 22):
+    for log2 in (18, 24):
         for lf in (0.25, 0.5, 1.0, 2.0, 4.0):
             nk = int(lf * (1 << log2) * 28)
             pool = max(4096, int(nk / 28 * 1.5) + (1 << log2) // 4)
-            res = {}
-            for form in ("fused", "plain"):
-                st = L.Set(log2, pool)
+            gen.manual_seed(seed + log2 * 100 + int(lf * 8))
+            batches = []
+            for _ in range(nb):
+                u = torch.rand(n, device="cuda", generator=gen)
+                ty = torch.where(u < 0.4, 1, torch.where(u < 0.9, 0, 2)).to(torch.uint8)
+                ty, _ = torch.sort(ty)  # contains, insert, remove: type-sorted parts
+                idx = torch.randint(0, 2 * nk, (n,), device="cuda", generator=gen)
+                batches.append((ty, _perm32(torch, idx)))
+            cnt = [(int((b[0] == 0).sum()), int((b[0] == 1).sum())) for b in batches]
+            sample = _perm32(torch, torch.randint(0, 2 * nk, (1 << 20,), device="cuda",
+                                                  generator=gen))
+            res, outs, held = {}, {}, {}
+            for form in ("fused", "plain", "lslab"):
+                if form == "lslab":
+                    if not have_ref:
+                        continue
+                    # lslab's identity hash (hash.h:12-14): a bucket's slabs
+                    # never exceed ceil(its inserts / 31)
+                    per = torch.zeros(1 << log2, dtype=torch.int64, device="cuda")
+                    mask = (1 << log2) - 1
+                    for off in range(0, nk, 1 << 24):
+                        k = _perm32(torch, torch.arange(off, min(nk, off + (1 << 24)),
+                                                        device="cuda"))
+                        per += torch.bincount(k.to(torch.int64) & mask, minlength=1 << log2)
+                    for (ty, k), (c, ins) in zip(batches, cnt):
+                        per += torch.bincount(k[c:c + ins].to(torch.int64) & mask,
+                                              minlength=1 << log2)
+                    bound = int(torch.clamp((per + 30) // 31 - 1, min=0).sum()) + 64
+                    del per
+                    st = RefSet(log2, bound)
+                    tmp = torch.empty(1 << 24, dtype=torch.bool, device="cuda")
+                else:
+                    st = L.Set(log2, pool)
                 for off in range(0, nk, 1 << 24):
                     k = _perm32(torch, torch.arange(off, min(nk, off + (1 << 24)), device="cuda"))
-                    st.insert(k)
+                    if form == "lslab":
+                        st.insert(k, tmp[:k.numel()])
+                    else:
+                        st.insert(k)
                     del k
                 torch.cuda.synchronize()
-                gen.manual_seed(seed + log2 * 100 + int(lf * 8))
-                nb = args.warmup + args.steps
-                batches = []
-                for _ in range(nb):
-                    u = torch.rand(n, device="cuda", generator=gen)
-                    ty = torch.where(u < 0.4, 1, torch.where(u < 0.9, 0, 2)).to(torch.uint8)
-                    ty, _ = torch.sort(ty)  # contains, insert, remove: type-sorted parts
-                    idx = torch.randint(0, 2 * nk, (n,), device="cuda", generator=gen)
-                    batches.append((ty, _perm32(torch, idx)))
-                out = torch.empty(n, dtype=torch.bool, device="cuda")
-                cnt = [(int((b[0] == 0).sum()), int((b[0] == 1).sum())) for b in batches]
+                out = torch.empty((nb, n), dtype=torch.bool, device="cuda")
 
                 def step(i):
                     ty, k = batches[i]
+                    o = out[i]
                     if form == "fused":
-                        st.execute_fused(ty, k, out)
-                    else:
-                        c, ins = cnt[i]
-                        if c:
-                            st.contains(k[:c], out[:c])
-                        if ins:
-                            st.insert(k[c:c + ins], out[c:c + ins])
-                        if n - c - ins:
-                            st.remove(k[c + ins:], out[c + ins:])
+                        st.execute_fused(ty, k, o)
+                        return
+                    c, ins = cnt[i]
+                    if c:
+                        st.contains(k[:c], o[:c])
+                    if ins:
+                        st.insert(k[c:c + ins], o[c:c + ins])
+                    if n - c - ins:
+                        st.remove(k[c + ins:], o[c + ins:])
                 for i in range(args.warmup):
                     step(i)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1026,16 +1114,38 @@ def run_sets(args, world, rank, local):
                 e1.record()
                 torch.cuda.synchronize()
                 res[form] = round(args.steps * n / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)
-                res["status"] = res.get("status", 0) | st.status()
+                held_out = torch.empty(sample.numel(), dtype=torch.bool, device="cuda")
+                st.contains(sample, held_out)
+                torch.cuda.synchronize()
+                held[form] = held_out
+                outs[form] = out
+                if form != "lslab":
+                    res["status"] = res.get("status", 0) | st.status()
                 st.close()
-                del batches
+                del st
+            ident = bool(torch.equal(outs["fused"], outs["plain"]))
+            vs_ref = None
+            if "lslab" in outs:
+                a, r = outs["fused"], outs["lslab"]
+                same_contains = all(torch.equal(a[i, :c], r[i, :c]) for i, (c, _) in enumerate(cnt))
+                same_removes = all(int(a[i, c + ins:].sum()) == int(r[i, c + ins:].sum())
+                                   for i, (c, ins) in enumerate(cnt))
+                vs_ref = bool(same_contains and same_removes
+                              and torch.equal(held["fused"], held["lslab"]))
             points.append({"buckets_log2": log2, "keys_per_slot": lf, "keys": nk,
                            "head_mb": round((1 << log2) * 160 / 1e6, 1),
                            "fused_mops": res["fused"], "plain_mops": res["plain"],
+                           "lslab_mops": res.get("lslab"),
+                           "results_identical_fused_plain": ident
+                           and bool(torch.equal(held["fused"], held["plain"])),
+                           "results_match_lslab": vs_ref,
                            "device_status": res["status"]})
+            del outs, held, batches, sample
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps({"workload": "sets", "description": run_sets.__doc__.split(".")[0],
                           "batch_ops": n, "steps": args.steps, "points": points}), flush=True)
+    return points
 
 
 def run_probes(args, world, rank, local):

@@ -120,6 +120,13 @@ typedef struct lsb_tuning {
                              warp serves its lanes' distinct keys one at a time, lanes
                              reading a slab's slots together); 0 = one op per thread,
                              tag sector then candidate slot (default, faster) */
+  uint32_t overlap;       /* mixed batches (execute, execute_fused): 1 = each window runs
+                             as launches on two streams, the reads through the lean read
+                             kernel while the mutations are listed, probed, grouped and
+                             ordered on a higher-priority stream; the mutations are applied
+                             after both (read-mostly windows of many ops); 0 = per-phase
+                             launches on the caller's stream (execute) and the persistent
+                             kernel (execute_fused) */
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */

@@ -62,6 +62,7 @@ class Tuning(C.Structure):
         ("fused_split", C.c_uint32),
         ("region_order", C.c_uint32),
         ("warp_probe", C.c_uint32),
+        ("overlap", C.c_uint32),
     ]
 
 

@@ -56,8 +56,10 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_FUSED_LEAN_READS
 #define LSB_FUSED_LEAN_READS 1
 #endif
+// two read lookups in flight per thread in the fused kernel's lean read
+// loop: measured slower at the 64-register cap (more spills), so off
 #ifndef LSB_FUSED_READ_PAIR
-#define LSB_FUSED_READ_PAIR 1
+#define LSB_FUSED_READ_PAIR 0
 #endif
 template <class Tr, bool kGroup, int P>
 __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
@@ -67,8 +69,42 @@ __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
   phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
 }
 
+// Windows run as launches on two streams (Table::run_plain, tuning overlap)
+// take their epochs from the device counter of the fused path, so a CUDA
+// graph of them can be replayed: every kernel of the window reads the
+// counter f (written only by the window's last block, in k_resolve) and uses
+// epoch 2f+1, or 1 after the tables were cleared when the epochs ran out.
+__device__ __forceinline__ uint32_t dev_window_slot(const uint32_t* fused_epoch) {
+  const uint32_t f = ld_cg_u32(fused_epoch);
+  return f + 1 > kFusedEpochs ? 0u : f;
+}
+
+// The two steps of a window's mutation probe when its reads run beside it
+// in k_read: the mutations are listed in op-index order (after clearing the
+// group and chunk tables if the epochs ran out: nothing reads them during
+// this kernel), then probed and grouped from the list by every warp.
+template <class Tr>
+__global__ void __launch_bounds__(256) k_list_muts(Scratch sc, Window<Tr> w,
+                                                   const uint32_t* fused_epoch) {
+  if (ld_cg_u32(fused_epoch) + 1 > kFusedEpochs) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nt = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i <= sc.gmask; i += nt) sc.gtab[i] = 0;
+    for (size_t i = tid; i <= sc.cmask; i += nt) sc.ctab[i] = 0;
+  }
+  phase_list_muts<Tr>(sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5);
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(512, 2 * LSB_PROBE_MIN_BLOCKS)
+    k_probe_list(TableView t, Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
+  w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
+  phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
+}
+
 // Read-only batch (get / contains) in its lean form: one op per thread, no
-// grouping, no work claims, the result written straight out.  The code is
+// grouping, no work claims, the result written straight out; with `types`,
+// the reads of a mixed window (other ops are left to the engine).  The code is
 // kept within 32 registers a thread (launch bound 256 x 8), so 2048 threads
 // fit an SM: a lookup is two dependent loads (meta sector, then the
 // candidate slot), latency-bound, and twice the resident warps keep twice
@@ -76,10 +112,12 @@ __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
 // candidate or a longer chain continues in find_rest.
 template <class Tr>
 __global__ void __launch_bounds__(256, 8)
-    k_read(TableView t, const typename Tr::Key* keys, void* out, uint32_t out_kind, uint32_t n) {
+    k_read(TableView t, const uint8_t* types, const typename Tr::Key* keys, void* out,
+           uint32_t out_kind, uint32_t n) {
   using Key = typename Tr::Key;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (types != nullptr && __ldcs(types + i) != kOpRead) return;
   Key key;
   if constexpr (sizeof(Key) == 8)
     key = (Key)ld_cs_u64(keys + i);
@@ -177,9 +215,12 @@ __global__ void __launch_bounds__(256)
 // Ordering of the window's big groups; when hot keys produced groups of
 // more than kSortSmall members, the grid (a cooperative launch) continues
 // with the huge_* steps between grid barriers.
+// fused_epoch: the window's epoch is the device one (see dev_window_slot).
 template <class Tr>
-__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar) {
+__global__ void __launch_bounds__(1024, 1)
+    k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar, const uint32_t* fused_epoch) {
   extern __shared__ uint32_t smem[];
+  if (fused_epoch != nullptr) w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe kernel has ended
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
@@ -194,14 +235,17 @@ __global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, Grid
 }
 
 // Last kernel of a per-phase window: it also leaves the counter block zeroed
-// for the next launch.
+// for the next launch.  With fused_epoch (a window on the device epoch), its
+// last block also advances the epoch counter.
 template <class Tr>
 __global__ void __launch_bounds__(1024, 1)
-    k_resolve(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar) {
+    k_resolve(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar, uint32_t* fused_epoch) {
   const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
+  const uint32_t slot = fused_epoch != nullptr ? dev_window_slot(fused_epoch) : 0u;
+  if (fused_epoch != nullptr) w.epoch = 2 * slot + 1;
   phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
   phase_resolve_reads<Tr>(sc, w, tid, nt);
-  release_counters(sc.cnt, bar, nullptr, 0);
+  release_counters(sc.cnt, bar, nullptr, 0, fused_epoch, slot + 1);
 }
 
 // One batch split into windows, all phases of all windows in one cooperative
@@ -801,13 +845,14 @@ struct Tuning {
   uint32_t prefetch = 0; // extra lookups in flight per thread (0..2)
   uint32_t dedup = 0;
   uint32_t warp_probe = 0;  // read-only batches through k_read_coop
+  uint32_t overlap = 0;     // mixed windows: reads in k_read beside the mutation steps
 };
 
 inline bool tuning_ok(const lsb_tuning& x) {
   return (x.block_threads == 128 || x.block_threads == 256 || x.block_threads == 512 ||
           x.block_threads == 1024) &&
          x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
-         x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1;
+         x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1 && x.overlap <= 1;
 }
 
 template <class Tr>
@@ -834,6 +879,10 @@ struct Table {
   uint32_t* fused_epoch = nullptr;  // device counter of fused windows (see k_fused)
   bool binned = false;         // fused path probes in table-region order (measured slower)
   int fused_per_sm[3][4] = {};  // occupancy by (prefetch, block size) once queried
+  // tuning overlap: the mutation steps of a window run on `side` (highest
+  // stream priority, so its blocks take SMs as k_read's blocks retire)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
   TableView view() const {
     TableView v;
@@ -854,6 +903,9 @@ struct Table {
                     sc.cnt, sc.obin, sc.perm, sc.clist, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
                     sc.lnu, sc.rnu, trace, fused_epoch};
     for (void* p : ptrs) cudaFree(p);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   int init(unsigned log2_buckets, const lsb_options* opt) {
@@ -940,6 +992,11 @@ struct Table {
                                 kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
+    int least = 0, greatest = 0;
+    LSB_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    LSB_CK(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
+    LSB_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    LSB_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     return LSB_OK;
   }
 
@@ -950,6 +1007,7 @@ struct Table {
     tune.prefetch = x.prefetch;
     tune.dedup = x.dedup;
     tune.warp_probe = x.warp_probe;
+    tune.overlap = x.overlap;
     split_q16 = (uint32_t)(((uint64_t)x.fused_split << 16) / 100);
     binned = x.region_order != 0;
     return LSB_OK;
@@ -963,6 +1021,7 @@ struct Table {
     x->fused_split = (uint32_t)(((uint64_t)split_q16 * 100 + 32768) >> 16);
     x->region_order = binned ? 1u : 0u;
     x->warp_probe = tune.warp_probe;
+    x->overlap = tune.overlap;
   }
 
   // Epoch of the next per-phase window (even: 2, 4, ...; the fused path uses
@@ -1028,7 +1087,7 @@ struct Table {
           k_read_coop<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), keys + off, o,
                                                           out ? out_kind : kOutNone, m);
         else
-          k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), keys + off, o,
+          k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), nullptr, keys + off, o,
                                                      out ? out_kind : kOutNone, m);
         LSB_CK(cudaGetLastError());
       }
@@ -1064,32 +1123,60 @@ struct Table {
       Window<Tr> w = window(types ? types + off : nullptr, uniform, keys + off * kstride, kstride,
                             v, vstride, out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr,
                             out_kind, m, v32);
-      int e = next_plain_epoch(s, &w.epoch);
-      if (e) return e;
+      const bool overlap = types != nullptr && tune.overlap && !tune.dedup &&
+                           lock_mode != kLockRW && kstride == 1 && out_kind != kOutOld &&
+                           out_kind != kOutOld32;
+      if (!overlap) {
+        int e = next_plain_epoch(s, &w.epoch);
+        if (e) return e;
+      }
       w.cnt = &sc.cnt[0];
       // the counters and the sort launch's grid barrier are zero here: the
       // previous launch's last block cleared them (release_counters)
-      const int grid = grid_for(m);
-      launch_probe<true>(grid, w, s);
-      {
-        GridBarrier* b = bar;
-        void* args[] = {&sc, &w, &b};
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(num_sms);
-        cfg.blockDim = dim3(256);
-        cfg.dynamicSmemBytes = kSortSmemBytes;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_sort<Tr>, args));
+      uint32_t* dev_epoch = overlap ? fused_epoch : nullptr;
+      if (overlap) {
+        // Reads write their results at probe time and never join a group;
+        // only reads after a same-key mutation are rewritten by the resolve
+        // step.  So the window's reads go through k_read on `s` while the
+        // mutations are listed, probed, grouped and ordered on `side`; the
+        // resolve step (the only one that writes the table) waits for both.
+        LSB_CK(cudaEventRecord(ev_fork, s));
+        LSB_CK(cudaStreamWaitEvent(side, ev_fork, 0));
+        const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
+        k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256, 0,
+                          side>>>(sc, w, fused_epoch);
+        k_probe_list<Tr><<<num_sms, 512, 0, side>>>(view(), sc, w, fused_epoch);
+        if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
+        LSB_CK(cudaEventRecord(ev_join, side));
+        k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), w.types, w.keys, w.out, w.out_kind, m);
+        LSB_CK(cudaStreamWaitEvent(s, ev_join, 0));
+      } else {
+        launch_probe<true>(grid_for(m), w, s);
+        if (int e2 = launch_sort(w, s, nullptr)) return e2;
       }
       const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
-      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar);
+      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar, dev_epoch);
       LSB_CK(cudaGetLastError());
     }
+    return LSB_OK;
+  }
+
+  // Ordering of the window's big groups (k_sort, a cooperative launch: its
+  // hot-key steps have grid barriers).
+  int launch_sort(Window<Tr> w, cudaStream_t s, const uint32_t* dev_epoch) {
+    GridBarrier* b = bar;
+    void* args[] = {&sc, &w, &b, &dev_epoch};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(num_sms);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = kSortSmemBytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_sort<Tr>, args));
     return LSB_OK;
   }
 
@@ -1111,6 +1198,9 @@ struct Table {
                 const uint64_t* vals, void* out, uint32_t out_kind, size_t n, cudaStream_t s) {
     if (n == 0) return LSB_OK;
     if (n > 0xFFFFFFFFull) return LSB_ERR_ARG;
+    // windows as launches on two streams (reads beside the mutation steps)
+    if (tune.overlap && types != nullptr && !tune.dedup && lock_mode != kLockRW)
+      return run_plain(types, uniform, keys, 1, vals, 1, out, out_kind, n, s);
     FusedJob<Tr> job;
     job.base = window(types, uniform, keys, 1, vals, 1, out, out_kind, (uint32_t)n);
     job.window = sc.max_window;
@@ -1309,6 +1399,7 @@ int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::K
     for (uint32_t prefetch : {0u, 1u, 2u}) {
       for (uint32_t cand = 0; cand < 1 + sizeof(kChunks) / sizeof(kChunks[0]); ++cand) {
         lsb_tuning c = cur;
+        c.overlap = 0;
         c.block_threads = block;
         c.prefetch = prefetch;
         c.fused_split = cand == 0 ? 0u : 100u;
@@ -1335,6 +1426,30 @@ int autotune(Table<Tr>& tb, int kind, const uint8_t* types, const typename Tr::K
       if (err) break;
     }
     if (err) break;
+  }
+  // the best shape with the two-stream window form (it uses the persistent
+  // kernel's shape only where the form does not apply)
+  if (!err && !cur.dedup && tb.lock_mode != kLockRW) {
+    lsb_tuning c = win;
+    c.overlap = 1;
+    if (tb.set_tuning(c) == LSB_OK) {
+      err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);  // warm-up
+      float t[kReps];
+      for (int r = 0; r < kReps && !err; ++r) {
+        cudaEventRecord(e0, s);
+        err = tb.run_fused(types, kOpRead, keys, vals, out, out_kind, n, s);
+        cudaEventRecord(e1, s);
+        if (!err && cudaEventSynchronize(e1) != cudaSuccess) err = LSB_ERR_CUDA;
+        if (!err) cudaEventElapsedTime(&t[r], e0, e1);
+      }
+      if (!err) {
+        std::sort(t, t + kReps);
+        if (t[kReps / 2] < best_ms) {
+          best_ms = t[kReps / 2];
+          win = c;
+        }
+      }
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -1287,7 +1287,8 @@ __device__ void huge_runs(const Scratch& sc, const Window<Tr>& w, uint32_t* smem
 // clears it for the next launch, so no memset launch precedes a batch.
 // Every thread of every block calls this once, as the block's last action.
 __device__ inline void release_counters(WinCounters* cnt, GridBarrier* bar, void* bins,
-                                        uint32_t bin_words) {
+                                        uint32_t bin_words, uint32_t* epoch_out = nullptr,
+                                        uint32_t epoch_next = 0) {
   __syncthreads();
   int last = 0;
   if (threadIdx.x == 0) {
@@ -1301,6 +1302,7 @@ __device__ inline void release_counters(WinCounters* cnt, GridBarrier* bar, void
     uint32_t* b = static_cast<uint32_t*>(bins);
     for (uint32_t i = threadIdx.x; b && i < bin_words; i += blockDim.x) b[i] = 0;
     if (threadIdx.x == 0) bar->count = 0;
+    if (threadIdx.x == 0 && epoch_out != nullptr) *epoch_out = epoch_next;
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
