@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--serve-loads", default="0.1,0.3,0.5,0.7,0.9,1.0",
                     help="serving: offered loads as fractions of the measured peak")
     ap.add_argument("--nbatches", type=int, default=4096)
+    ap.add_argument("--set-log2", default="18,24", help="sets: table sizes (log2 buckets)")
+    ap.add_argument("--set-lf", default="0.25,0.5,1,2,4", help="sets: keys per head-slab slot")
+    ap.add_argument("--set-forms", default="fused,plain,lslab", help="sets: forms to run")
     ap.add_argument("--no-autotune", action="store_true",
                     help="zipf9505 and batches: library-default (or --block/--chunk/...) "
                          "tuning instead of the autotuner")
@@ -407,6 +410,27 @@ def run_ours(args, world, rank, local):
             break
     st = fused.status() | plain.status()
 
+    # ---- random-probe ceiling: the accesses of each timed batch's gets at
+    # uniformly random keys of the same table, nothing else
+    # (lsb_probe_calibrate over the table's head slabs)
+    view = fused.device_view()
+    cal_out = torch.empty((n, 2), dtype=torch.int64, device="cuda")
+    for b in range(args.warmup):
+        L.probe_calibrate(view["slabs"], 1 << args.buckets_log2, 480, d_keys[b][:n_get[b]],
+                          cal_out, seed=b)
+    cev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    cev[0].record(stream)
+    for s in range(args.steps):
+        b = args.warmup + s
+        L.probe_calibrate(view["slabs"], 1 << args.buckets_log2, 480, d_keys[b][:n_get[b]],
+                          cal_out, seed=b)
+    cev[1].record(stream)
+    torch.cuda.synchronize()
+    cal_ms = max_over_ranks(cev[0].elapsed_time(cev[1]), world)
+    cal_gets = sum(n_get[args.warmup:])
+    del cal_out
+
     # ---- e2e through the public API with host buffers
     h_types = [torch.from_numpy(b.types).pin_memory() for b in batches]
     h_keys = [torch.from_numpy(b.keys.view(np.int64)).pin_memory() for b in batches]
@@ -575,7 +599,15 @@ def run_ours(args, world, rank, local):
                                         "2^20-op batch of this workload (committed capture, "
                                         "not this run)"),
                      "peak_kind": f"{peak_kind} copy bandwidth",
-                     "alg_bytes_per_op": round(statistics.mean(ab) / n, 2)},
+                     "alg_bytes_per_op": round(statistics.mean(ab) / n, 2),
+                     "gather_ceiling": {
+                         "gets_mops": round(cal_gets / (cal_ms * 1e-3) / 1e6, 1),
+                         "batch_floor_us": round(cal_ms * 1e3 / args.steps, 2),
+                         "frac": round(cal_ms / fused_ms, 4),
+                         "what": ("the accesses of each batch's gets at uniformly random keys "
+                                  "of the same 2^%d-bucket table and nothing else (meta sector, "
+                                  "then a slot of the same slab; lsb_probe_calibrate); frac = "
+                                  "that time / the batch's time" % args.buckets_log2)}},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1044,8 +1076,9 @@ def run_sets(args, world, rank, local):
     nb = args.warmup + args.steps
     have_ref = oracle.ref_available()
     points = []
-    for log2 in (18, 24):
-        for lf in (0.25, 0.5, 1.0, 2.0, 4.0):
+    forms = [f for f in args.set_forms.split(",") if f]
+    for log2 in [int(x) for x in args.set_log2.split(",")]:
+        for lf in [float(x) for x in args.set_lf.split(",")]:
             nk = int(lf * (1 << log2) * 28)
             pool = max(4096, int(nk / 28 * 1.5) + (1 << log2) // 4)
             gen.manual_seed(seed + log2 * 100 + int(lf * 8))
@@ -1060,7 +1093,7 @@ def run_sets(args, world, rank, local):
             sample = _perm32(torch, torch.randint(0, 2 * nk, (1 << 20,), device="cuda",
                                                   generator=gen))
             res, outs, held = {}, {}, {}
-            for form in ("fused", "plain", "lslab"):
+            for form in forms:
                 if form == "lslab":
                     if not have_ref:
                         continue
@@ -1123,9 +1156,10 @@ def run_sets(args, world, rank, local):
                     res["status"] = res.get("status", 0) | st.status()
                 st.close()
                 del st
-            ident = bool(torch.equal(outs["fused"], outs["plain"]))
+            both = "fused" in outs and "plain" in outs
+            ident = bool(torch.equal(outs["fused"], outs["plain"])) if both else None
             vs_ref = None
-            if "lslab" in outs:
+            if "lslab" in outs and "fused" in outs:
                 a, r = outs["fused"], outs["lslab"]
                 same_contains = all(torch.equal(a[i, :c], r[i, :c]) for i, (c, _) in enumerate(cnt))
                 same_removes = all(int(a[i, c + ins:].sum()) == int(r[i, c + ins:].sum())
@@ -1134,12 +1168,12 @@ def run_sets(args, world, rank, local):
                               and torch.equal(held["fused"], held["lslab"]))
             points.append({"buckets_log2": log2, "keys_per_slot": lf, "keys": nk,
                            "head_mb": round((1 << log2) * 160 / 1e6, 1),
-                           "fused_mops": res["fused"], "plain_mops": res["plain"],
+                           "fused_mops": res.get("fused"), "plain_mops": res.get("plain"),
                            "lslab_mops": res.get("lslab"),
-                           "results_identical_fused_plain": ident
-                           and bool(torch.equal(held["fused"], held["plain"])),
+                           "results_identical_fused_plain": (ident and bool(torch.equal(
+                               held["fused"], held["plain"]))) if both else None,
                            "results_match_lslab": vs_ref,
-                           "device_status": res["status"]})
+                           "device_status": res.get("status", 0)})
             del outs, held, batches, sample
             torch.cuda.empty_cache()
     if rank == 0:

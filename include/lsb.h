@@ -492,6 +492,19 @@ typedef struct lsb_table_view {
 int lsb_map_device_view(const lsb_map* m, lsb_table_view* out);
 int lsb_set_device_view(const lsb_set* s, lsb_table_view* out);
 
+/* ---- measuring ---------------------------------------------------------- */
+/* Probe-rate calibration (no reference counterpart): for i < n, read req[i],
+ * pick a slab of the array `slabs` (nslabs slabs of slab_bytes each)
+ * uniformly at random, load its 32-byte meta sector, then, dependent on it,
+ * one 16-byte slot of the same slab, and store 16 bytes to out[2i..2i+1]: the
+ * accesses of one get at a uniformly random key and nothing else.  Its rate
+ * is the ceiling that address translation and DRAM latency put on random
+ * lookups over an array of that size (pass a table's slab array from
+ * lsb_*_device_view; only reads it).  Async on `s`. */
+int lsb_probe_calibrate(const void* slabs, uint64_t nslabs, uint32_t slab_bytes,
+                        const uint64_t* req, uint64_t* out, size_t n, uint64_t seed,
+                        cudaStream_t s);
+
 /* ---- misc ------------------------------------------------------------- */
 const char* lsb_error_string(int code);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */

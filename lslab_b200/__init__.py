@@ -97,6 +97,13 @@ class _Table:
         _lib.check(getattr(lib(), f"lsb_{self._prefix}_{name}")(self._h, *args),
                    f"lsb_{self._prefix}_{name}")
 
+    def device_view(self) -> dict:
+        """The table's device handles (lsb_*_device_view): slab array pointer,
+        bucket mask, lock mode, ... as a dict of ints."""
+        v = _lib.TableView()
+        self._call("device_view", C.byref(v))
+        return {f: int(getattr(v, f) or 0) for f, _ in _lib.TableView._fields_}
+
     def close(self):
         if self._h is not None:
             getattr(lib(), f"lsb_{self._prefix}_destroy")(self._h)
@@ -210,6 +217,15 @@ class _Table:
         cur.update(kw)
         t = _lib.Tuning(**cur)
         self._call("set_tuning", C.byref(t))
+
+
+def probe_calibrate(slabs: int, nslabs: int, slab_bytes: int, req, out, seed: int = 0,
+                    size=None, stream=None) -> None:
+    """lsb_probe_calibrate: the accesses of one get at a uniformly random key
+    per element of `req` over a slab array (see include/lsb.h)."""
+    _lib.check(lib().lsb_probe_calibrate(int(slabs), int(nslabs), int(slab_bytes), _ptr(req),
+                                         _ptr(out), _len(req, size), int(seed) & (2**64 - 1),
+                                         _stream(stream)), "lsb_probe_calibrate")
 
 
 class Graph:

@@ -66,6 +66,21 @@ class Tuning(C.Structure):
     ]
 
 
+class TableView(C.Structure):
+    """lsb_table_view: the device-side handles of a table (include/lsb.h)."""
+    _fields_ = [
+        ("slabs", C.c_void_p),
+        ("locks", C.c_void_p),
+        ("status", C.c_void_p),
+        ("pool", C.c_void_p),
+        ("free_stack", C.c_void_p),
+        ("mask", C.c_uint32),
+        ("lock_mode", C.c_uint32),
+        ("chunk", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
 class ServeOptions(C.Structure):
     _fields_ = [
         ("max_wave_ops", C.c_uint32),
@@ -129,6 +144,7 @@ _SIGS = {
     "lsb_kvs_compact": (C.c_int, [_P, _P]),
     "lsb_map_device_view": (C.c_int, [_P, _P]),
     "lsb_set_device_view": (C.c_int, [_P, _P]),
+    "lsb_probe_calibrate": (C.c_int, [_P, _U64, C.c_uint32, _P, _P, _SZ, _U64, _P]),
     "lsb_map_get_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),
     "lsb_map_put_v32": (C.c_int, [_P, _P, _P, _P, _SZ, _P]),
     "lsb_map_put_pairs_v32": (C.c_int, [_P, _P, _P, _SZ, _P]),

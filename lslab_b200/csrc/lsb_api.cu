@@ -79,29 +79,6 @@ __device__ __forceinline__ uint32_t dev_window_slot(const uint32_t* fused_epoch)
   return f + 1 > kFusedEpochs ? 0u : f;
 }
 
-// The two steps of a window's mutation probe when its reads run beside it
-// in k_read: the mutations are listed in op-index order (after clearing the
-// group and chunk tables if the epochs ran out: nothing reads them during
-// this kernel), then probed and grouped from the list by every warp.
-template <class Tr>
-__global__ void __launch_bounds__(256) k_list_muts(Scratch sc, Window<Tr> w,
-                                                   const uint32_t* fused_epoch) {
-  if (ld_cg_u32(fused_epoch) + 1 > kFusedEpochs) {
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t nt = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = tid; i <= sc.gmask; i += nt) sc.gtab[i] = 0;
-    for (size_t i = tid; i <= sc.cmask; i += nt) sc.ctab[i] = 0;
-  }
-  phase_list_muts<Tr>(sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5);
-}
-
-template <class Tr>
-__global__ void __launch_bounds__(512, 2 * LSB_PROBE_MIN_BLOCKS)
-    k_probe_list(TableView t, Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
-  w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
-  phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
-}
-
 // Read-only batch (get / contains) in its lean form: one op per thread, no
 // grouping, no work claims, the result written straight out; with `types`,
 // the reads of a mixed window (other ops are left to the engine).  The code is
@@ -215,12 +192,9 @@ __global__ void __launch_bounds__(256)
 // Ordering of the window's big groups; when hot keys produced groups of
 // more than kSortSmall members, the grid (a cooperative launch) continues
 // with the huge_* steps between grid barriers.
-// fused_epoch: the window's epoch is the device one (see dev_window_slot).
 template <class Tr>
-__global__ void __launch_bounds__(1024, 1)
-    k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar, const uint32_t* fused_epoch) {
+__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar) {
   extern __shared__ uint32_t smem[];
-  if (fused_epoch != nullptr) w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe kernel has ended
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
@@ -231,6 +205,43 @@ __global__ void __launch_bounds__(1024, 1)
   if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
   huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
   if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_runs<Tr>(sc, w, smem, gtid, gthreads);
+}
+
+// The mutation steps of a window whose reads run beside it in k_read (the
+// two-stream form, tuning overlap), in one cooperative launch of one
+// 256-thread block per SM, launched first so its blocks are resident before
+// the read kernel takes the rest of each SM: clear the group and chunk
+// tables if the device epochs ran out, list the mutations in op-index order,
+// probe and group them from the list, order the big groups (hot keys by the
+// multi-step grid algorithm), with grid barriers between the steps.  Reads
+// are neither probed nor resolved here.
+template <class Tr>
+__global__ void __launch_bounds__(256, 4)
+    k_mutations(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar,
+                const uint32_t* fused_epoch) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t f = ld_cg_u32(fused_epoch);
+  w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const uint32_t warp = spread_warp(), nwarps = gthreads >> 5;
+  uint32_t seq = 0;
+  if (f + 1 > kFusedEpochs) {  // grid-uniform: every block read the same counter
+    for (size_t i = gtid; i <= sc.gmask; i += gthreads) sc.gtab[i] = 0;
+    for (size_t i = gtid; i <= sc.cmask; i += gthreads) sc.ctab[i] = 0;
+  }
+  phase_list_muts<Tr>(sc, w, warp, nwarps);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  phase_probe_list<Tr>(t, sc, w, warp, nwarps, false);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  phase_sort_big<Tr>(sc, w, smem);
+  if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe step has ended
+  huge_hist<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  huge_scan<Tr>(sc, w, smem);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
   huge_runs<Tr>(sc, w, smem, gtid, gthreads);
 }
 
@@ -986,6 +997,8 @@ struct Table {
     bins = reinterpret_cast<BinCounters*>(reinterpret_cast<uint8_t*>(sc.cnt) + kBinsOffset);
     LSB_CK(cudaFuncSetAttribute(k_sort<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
+    LSB_CK(cudaFuncSetAttribute(k_mutations<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1137,22 +1150,36 @@ struct Table {
       if (overlap) {
         // Reads write their results at probe time and never join a group;
         // only reads after a same-key mutation are rewritten by the resolve
-        // step.  So the window's reads go through k_read on `s` while the
-        // mutations are listed, probed, grouped and ordered on `side`; the
-        // resolve step (the only one that writes the table) waits for both.
+        // step, which is also the only step that writes the table.  So the
+        // window's reads go through k_read on `s` while the mutation steps
+        // run in k_mutations on `side` (launched first: its one block per SM
+        // is resident before k_read fills the SMs); the resolve step waits
+        // for both.
         LSB_CK(cudaEventRecord(ev_fork, s));
         LSB_CK(cudaStreamWaitEvent(side, ev_fork, 0));
-        const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
-        k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256, 0,
-                          side>>>(sc, w, fused_epoch);
-        k_probe_list<Tr><<<num_sms, 512, 0, side>>>(view(), sc, w, fused_epoch);
-        if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
+        {
+          TableView tv = view();
+          GridBarrier* b = bar;
+          uint32_t* fe = fused_epoch;
+          void* args[] = {&tv, &sc, &w, &b, &fe};
+          cudaLaunchConfig_t cfg = {};
+          cfg.gridDim = dim3(num_sms);
+          cfg.blockDim = dim3(256);
+          cfg.dynamicSmemBytes = kSortSmemBytes;
+          cfg.stream = side;
+          cudaLaunchAttribute attr[1];
+          attr[0].id = cudaLaunchAttributeCooperative;
+          attr[0].val.cooperative = 1;
+          cfg.attrs = attr;
+          cfg.numAttrs = 1;
+          LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_mutations<Tr>, args));
+        }
         LSB_CK(cudaEventRecord(ev_join, side));
         k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), w.types, w.keys, w.out, w.out_kind, m);
         LSB_CK(cudaStreamWaitEvent(s, ev_join, 0));
       } else {
         launch_probe<true>(grid_for(m), w, s);
-        if (int e2 = launch_sort(w, s, nullptr)) return e2;
+        if (int e2 = launch_sort(w, s)) return e2;
       }
       const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
       k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar, dev_epoch);
@@ -1163,9 +1190,9 @@ struct Table {
 
   // Ordering of the window's big groups (k_sort, a cooperative launch: its
   // hot-key steps have grid barriers).
-  int launch_sort(Window<Tr> w, cudaStream_t s, const uint32_t* dev_epoch) {
+  int launch_sort(Window<Tr> w, cudaStream_t s) {
     GridBarrier* b = bar;
-    void* args[] = {&sc, &w, &b, &dev_epoch};
+    void* args[] = {&sc, &w, &b};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(num_sms);
     cfg.blockDim = dim3(256);

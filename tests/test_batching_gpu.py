@@ -113,7 +113,8 @@ def test_autotune_keeps_single_application_state(cuda):
     m = L.Map(log2, max_window=1 << 15)
     out = results_buf(len(keys))
     best = m.autotune(dev(types), dev(keys), dev(vals), out)
-    assert best["block_threads"] in (256, 512, 1024)
+    assert best["block_threads"] in (128, 256, 512, 1024)
+    assert best["overlap"] in (0, 1)
     assert best["prefetch"] in (0, 1, 2)
     assert m.tuning() == best
     k, v = m.dump()
