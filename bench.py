@@ -640,14 +640,18 @@ def side_workloads(args, world, rank, local) -> dict:
                                               "plain_issue", "plain_python_mops",
                                               "results_identical", "ops", "batches",
                                               "device_status")}
-    sv = run_serving(side, world, rank, local)
-    at70 = [p for p in sv["sweep"] if abs(p["load"] - 0.7) < 1e-9]
-    out["serving"] = {
-        "peak_mops": sv["peak_mops"], "wave_ops": sv["wave_ops"],
-        "at_70pct": at70[0] if at70 else None,
-        "p99_us_by_load": {str(p["load"]): p["p99_us"] for p in sv["sweep"]},
-        "loop_state": sv["loop"]["state"], "device_status": sv["device_status"],
-    }
+    # the serving loop at two wave limits: 2^16 ops (throughput) and 2^14
+    # (latency: smaller waves, lower peak)
+    for key, wave in (("serving", 1 << 16), ("serving_wave_2e14", 1 << 14)):
+        side.wave_ops = wave
+        sv = run_serving(side, world, rank, local)
+        at70 = [p for p in sv["sweep"] if abs(p["load"] - 0.7) < 1e-9]
+        out[key] = {
+            "peak_mops": sv["peak_mops"], "wave_ops": sv["wave_ops"],
+            "at_70pct": at70[0] if at70 else None,
+            "p99_us_by_load": {str(p["load"]): p["p99_us"] for p in sv["sweep"]},
+            "loop_state": sv["loop"]["state"], "device_status": sv["device_status"],
+        }
     return out
 
 

@@ -56,6 +56,19 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_FUSED_LEAN_READS
 #define LSB_FUSED_LEAN_READS 1
 #endif
+// Two-stream window form (tuning overlap): LSB_OVERLAP_SPLIT 1 = the mutation
+// steps as three kernels (list, probe from the list, ordering), 0 = one
+// cooperative kernel; LSB_OVERLAP_READ_BLOCKS = read-kernel blocks per SM
+// (a grid-stride grid that leaves room on every SM for the mutation steps;
+// 0 = one thread per op).  Measured on the 2^20-op 95/5 batch (per batch):
+// 1/0 75.8 us, 1/4 78.6, 1/6 81.8, 1/7 79.6, 0/6 101.9; per-op-type calls
+// 77.8 us.
+#ifndef LSB_OVERLAP_SPLIT
+#define LSB_OVERLAP_SPLIT 1
+#endif
+#ifndef LSB_OVERLAP_READ_BLOCKS
+#define LSB_OVERLAP_READ_BLOCKS 0
+#endif
 // two read lookups in flight per thread in the fused kernel's lean read
 // loop: measured slower at the 64-register cap (more spills), so off
 #ifndef LSB_FUSED_READ_PAIR
@@ -92,24 +105,25 @@ __global__ void __launch_bounds__(256, 8)
     k_read(TableView t, const uint8_t* types, const typename Tr::Key* keys, void* out,
            uint32_t out_kind, uint32_t n) {
   using Key = typename Tr::Key;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (types != nullptr && __ldcs(types + i) != kOpRead) return;
-  Key key;
-  if constexpr (sizeof(Key) == 8)
-    key = (Key)ld_cs_u64(keys + i);
-  else
-    key = (Key)ld_cs_u32(keys + i);
-  uint64_t val;
-  const bool found = read_lookup<Tr>(t, key, &val);
-  if (out_kind == kOutResult) {
-    uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
-    st_cs_u64(p, found ? 1ull : 0ull);
-    st_cs_u64(p + 1, found ? val : 0ull);
-  } else if (out_kind == kOutResult32) {
-    st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
-  } else if (out_kind == kOutBool) {
-    st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+  // one op per thread with a grid of n threads; a smaller grid strides
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (types != nullptr && __ldcs(types + i) != kOpRead) continue;
+    Key key;
+    if constexpr (sizeof(Key) == 8)
+      key = (Key)ld_cs_u64(keys + i);
+    else
+      key = (Key)ld_cs_u32(keys + i);
+    uint64_t val;
+    const bool found = read_lookup<Tr>(t, key, &val);
+    if (out_kind == kOutResult) {
+      uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
+      st_cs_u64(p, found ? 1ull : 0ull);
+      st_cs_u64(p + 1, found ? val : 0ull);
+    } else if (out_kind == kOutResult32) {
+      st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
+    } else if (out_kind == kOutBool) {
+      st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+    }
   }
 }
 
@@ -192,9 +206,12 @@ __global__ void __launch_bounds__(256)
 // Ordering of the window's big groups; when hot keys produced groups of
 // more than kSortSmall members, the grid (a cooperative launch) continues
 // with the huge_* steps between grid barriers.
+// fused_epoch: the window's epoch is the device one (the two-stream form).
 template <class Tr>
-__global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar) {
+__global__ void __launch_bounds__(1024, 1)
+    k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar, const uint32_t* fused_epoch) {
   extern __shared__ uint32_t smem[];
+  if (fused_epoch != nullptr) w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe kernel has ended
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
@@ -206,6 +223,28 @@ __global__ void __launch_bounds__(1024, 1) k_sort(Scratch sc, Window<Tr> w, Grid
   huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
   if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
   huge_runs<Tr>(sc, w, smem, gtid, gthreads);
+}
+
+// The mutation steps of the two-stream form as separate kernels of 256-thread
+// blocks (LSB_OVERLAP_SPLIT 1): list, then probe and group from the list;
+// the ordering is k_sort.  The window's epoch is the device one.
+template <class Tr>
+__global__ void __launch_bounds__(256) k_list_muts(Scratch sc, Window<Tr> w,
+                                                   const uint32_t* fused_epoch) {
+  if (ld_cg_u32(fused_epoch) + 1 > kFusedEpochs) {  // epochs ran out: clear the tables
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nt = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i <= sc.gmask; i += nt) sc.gtab[i] = 0;
+    for (size_t i = tid; i <= sc.cmask; i += nt) sc.ctab[i] = 0;
+  }
+  phase_list_muts<Tr>(sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5);
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(256, 4)
+    k_probe_list(TableView t, Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
+  w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
+  phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
 }
 
 // The mutation steps of a window whose reads run beside it in k_read (the
@@ -1157,7 +1196,13 @@ struct Table {
         // for both.
         LSB_CK(cudaEventRecord(ev_fork, s));
         LSB_CK(cudaStreamWaitEvent(side, ev_fork, 0));
-        {
+        if (LSB_OVERLAP_SPLIT) {
+          const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
+          k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256,
+                            0, side>>>(sc, w, fused_epoch);
+          k_probe_list<Tr><<<num_sms * 2, 256, 0, side>>>(view(), sc, w, fused_epoch);
+          if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
+        } else {
           TableView tv = view();
           GridBarrier* b = bar;
           uint32_t* fe = fused_epoch;
@@ -1175,11 +1220,16 @@ struct Table {
           LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_mutations<Tr>, args));
         }
         LSB_CK(cudaEventRecord(ev_join, side));
-        k_read<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), w.types, w.keys, w.out, w.out_kind, m);
+        const uint32_t rblocks = LSB_OVERLAP_READ_BLOCKS
+                                     ? std::min<uint32_t>((m + 255) / 256,
+                                                          num_sms * LSB_OVERLAP_READ_BLOCKS)
+                                     : (m + 255) / 256;
+        k_read<Tr><<<std::max(1u, rblocks), 256, 0, s>>>(view(), w.types, w.keys, w.out,
+                                                          w.out_kind, m);
         LSB_CK(cudaStreamWaitEvent(s, ev_join, 0));
       } else {
         launch_probe<true>(grid_for(m), w, s);
-        if (int e2 = launch_sort(w, s)) return e2;
+        if (int e2 = launch_sort(w, s, nullptr)) return e2;
       }
       const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
       k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar, dev_epoch);
@@ -1190,9 +1240,9 @@ struct Table {
 
   // Ordering of the window's big groups (k_sort, a cooperative launch: its
   // hot-key steps have grid barriers).
-  int launch_sort(Window<Tr> w, cudaStream_t s) {
+  int launch_sort(Window<Tr> w, cudaStream_t s, const uint32_t* dev_epoch) {
     GridBarrier* b = bar;
-    void* args[] = {&sc, &w, &b};
+    void* args[] = {&sc, &w, &b, &dev_epoch};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(num_sms);
     cfg.blockDim = dim3(256);

@@ -936,25 +936,32 @@ __device__ void sort_group_block(const Scratch& sc, const Window<Tr>& w, uint32_
 }
 
 // A group of kInline+1 .. kWarpSort members, ordered by one warp: each lane
-// holds members lane and lane+32 and ranks them against all others by
-// shuffles, tracking its predecessor (the largest smaller index) on the way.
-template <class Tr>
-__device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t gslot, uint32_t c,
-                                uint32_t off, bool upd) {
+// holds members lane + 32h (h < K) and ranks them against all others by
+// shuffles, tracking each one's predecessor (the largest smaller index) on
+// the way (32 K^2 compares a lane).
+template <class Tr, int K>
+__device__ void sort_group_warp_k(const Scratch& sc, const Window<Tr>& w, uint32_t gslot,
+                                  uint32_t c, uint32_t off, bool upd) {
   const uint32_t lane = lane_id();
-  uint32_t x[2];
+  uint32_t x[K];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int h = 0; h < K; ++h) {
     const uint32_t j = lane + 32 * h;
     x[h] = j < c ? member_at(sc, w.epoch, gslot, j) : 0xFFFFFFFFu;
   }
-  uint32_t rank[2] = {0, 0}, pred[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
+  uint32_t rank[K], pred[K];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int g = 0; g < K; ++g) {
+    rank[g] = 0;
+    pred[g] = 0xFFFFFFFFu;
+  }
+#pragma unroll
+  for (int h = 0; h < K; ++h) {
+    if (32u * h >= c) break;  // warp-uniform
     for (uint32_t q = 0; q < 32; ++q) {
       const uint32_t y = __shfl_sync(0xFFFFFFFFu, x[h], q);
 #pragma unroll
-      for (int g = 0; g < 2; ++g) {
+      for (int g = 0; g < K; ++g) {
         if (32 * h + q < c && y < x[g]) {
           ++rank[g];
           if (pred[g] == 0xFFFFFFFFu || y > pred[g]) pred[g] = y;
@@ -963,7 +970,7 @@ __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t
     }
   }
 #pragma unroll
-  for (int g = 0; g < 2; ++g) {
+  for (int g = 0; g < K; ++g) {
     const uint32_t j = lane + 32 * g;
     if (j < c && x[g] < w.n) {
       sc.seg[off + rank[g]] = x[g];
@@ -972,23 +979,37 @@ __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t
   }
   if (!upd) return;  // warp-uniform
   // lnu: the largest smaller member that is not an update
-  uint32_t nu_of[2];
+  uint32_t nu_of[K];
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
+  for (int h = 0; h < K; ++h)
     nu_of[h] = (x[h] < w.n && op_type(w, x[h]) != kOpUpdate) ? x[h] : 0xFFFFFFFFu;
-  uint32_t lnu[2] = {0, 0};  // 1 + member, 0 = none
+  uint32_t lnu[K];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
+  for (int g = 0; g < K; ++g) lnu[g] = 0;  // 1 + member, 0 = none
+#pragma unroll
+  for (int h = 0; h < K; ++h) {
+    if (32u * h >= c) break;  // warp-uniform
     for (uint32_t q = 0; q < 32; ++q) {
       const uint32_t y = __shfl_sync(0xFFFFFFFFu, nu_of[h], q);
 #pragma unroll
-      for (int g = 0; g < 2; ++g)
+      for (int g = 0; g < K; ++g)
         if (y != 0xFFFFFFFFu && y < x[g] && y + 1 > lnu[g]) lnu[g] = y + 1;
     }
   }
 #pragma unroll
-  for (int g = 0; g < 2; ++g)
+  for (int g = 0; g < K; ++g)
     if (lane + 32 * g < c && x[g] < w.n) sc.lnu[x[g]] = lnu[g];
+}
+
+// Two members a lane: groups of up to 64.  (Four a lane, groups up to 128
+// with the block sort taking only larger ones, measured slower: the fused
+// kernel spilled more at its 64-register cap, 97 -> 103 us on the 2^20-op
+// 95/5 batch, and the serving loop's latency did not change.)
+template <class Tr>
+__device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t gslot, uint32_t c,
+                                uint32_t off, bool upd) {
+  static_assert(kWarpSort == 64, "one warp holds at most 2 members a lane");
+  sort_group_warp_k<Tr, 2>(sc, w, gslot, c, off, upd);
 }
 
 // Phase D: block b orders large groups b, b + gridDim.x, ... (the critical
