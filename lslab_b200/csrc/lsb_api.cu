@@ -328,7 +328,6 @@ __device__ __forceinline__ void trace_mark(uint64_t* tr, uint32_t& at, uint32_t 
 struct NoHook {
   static constexpr bool kActive = false;
   __device__ void operator()() const {}
-  __device__ void prefetch() const {}
 };
 
 // All windows of one batch.  `seq` counts the grid barriers this launch has
@@ -338,7 +337,7 @@ struct NoHook {
 template <class Tr, int P, bool kList = true, class Hook = NoHook>
 __device__ void fused_windows(const TableView& t, const Scratch& sc, const FusedJob<Tr>& job,
                               GridBarrier* bar, uint32_t* smem, uint32_t& seq,
-                              const Hook& hook = Hook{}, bool* hooked_in_sort = nullptr) {
+                              const Hook& hook = Hook{}) {
   const uint32_t nblocks = gridDim.x;
   // spread indices: small windows use many SMs; tid 0 is still thread 0 of block 0
   const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
@@ -426,16 +425,8 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
     const bool has_big = ld_cg_u32(&w.cnt->big_count) != 0;
     const bool has_mut = ld_cg_u32(&w.cnt->mut_count) != 0;
     const bool has_huge = huge_groups(sc, w.cnt) != 0;
-    // With a hook and an ordering step of warp- and block-sized groups only,
-    // the hook runs during that step (warp 0; block 0 takes no ordering
-    // work) and every block then runs its second part, so both leave the
-    // critical path of the resolve step.  Grid-uniform.
-    const bool hook_sort = Hook::kActive && wi + 1 == nwin && has_big && !has_huge && split >= w.n;
-    if (hooked_in_sort) *hooked_in_sort = hook_sort;
     if (has_big || split < w.n) {
-      if (hook_sort && tid < 32) hook();
-      if (has_big) phase_sort_big<Tr>(sc, w, smem, hook_sort);
-      if (hook_sort) hook.prefetch();
+      if (has_big) phase_sort_big<Tr>(sc, w, smem);
       if (has_huge) huge_hist<Tr>(sc, w, warp, nwarps);
       if (split < w.n && lean_reads && split == 0 && perm == nullptr)
         phase_read_lean<Tr, LSB_FUSED_READ_PAIR != 0>(t, w, &w.cnt->late_cursor, 0, w.n);
@@ -454,11 +445,10 @@ __device__ void fused_windows(const TableView& t, const Scratch& sc, const Fused
       if (!grid_barrier(bar, nblocks, t.status, seq)) return;
     }
     trace_mark(job.trace, tat, wi, 2);
-    // with a hook not run during the ordering step, warp 0 (threads 0..31 of
-    // block 0) runs it during the last window's resolve; it takes no resolve
-    // work either way
+    // with a hook, warp 0 (threads 0..31 of block 0) runs it during the last
+    // window's resolve and takes no resolve work
     const uint32_t r0 = Hook::kActive ? 32u : 0u;
-    if (Hook::kActive && wi + 1 == nwin && !hook_sort && tid < 32) hook();
+    if (Hook::kActive && wi + 1 == nwin && tid < 32) hook();
     if (has_mut && (!Hook::kActive || tid >= r0)) {
       // Mutations and the reads after the first mutation resolve
       // independently.  A small window (every thread holds at most one item
@@ -547,12 +537,10 @@ struct ServeJob {
   const uint64_t* a_vals;
   lsb_result* a_out;
   uint64_t arena_cap;
-  uint8_t* d_types;         // HBM working copies of waves' ops: two sets of
-  uint64_t* d_keys;         // max_wave_ops, the set of the descriptor index
+  uint8_t* d_types;         // HBM working copy of a wave's ops
+  uint64_t* d_keys;
   uint64_t* d_vals;
   WaveDesc* wave;           // two descriptors, alternating by admission
-  uint32_t* admit_seq;      // number of the last admission made by the hook
-  uint32_t* pf_cursor;      // claim cursor of the next wave's prefetch
   uint32_t max_wave_ops;
   uint32_t pad;
   uint64_t idle_ns;         // a blocking admission waits at most this long (%globaltimer)
@@ -733,27 +721,8 @@ __device__ void serve_admit(const TableView& t, const ServeJob& j, WaveDesc* out
   }
 }
 
-// The ops of wave-descriptor set `set` (n ops from arena position pos) into
-// that set's HBM working copy; .cv loads because the host rewrites arena
-// slots between waves; all three loads before any store: they cross PCIe
-// together.
-__device__ __forceinline__ void gather_op(const ServeJob& j, uint32_t set, uint64_t pos,
-                                          uint32_t i) {
-  const uint8_t ty = __ldcv(j.a_types + pos + i);
-  const uint64_t key = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos + i);
-  const uint64_t val = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos + i);
-  const size_t at = (size_t)set * j.max_wave_ops + i;
-  j.d_types[at] = ty;
-  j.d_keys[at] = key;
-  j.d_vals[at] = val;
-}
-
-// The serving loop's hook.  Warp 0 of block 0 admits the next wave
-// (non-blocking) during the current wave's ordering step, or its resolve
-// step when it has none, and announces it (admit_seq = admit_no).  Then every
-// block, once its own work of that step is done, copies a share of the
-// admitted wave's ops into the other working-copy set (block-wide claims of
-// blockDim ops), so the next wave starts without a gather step.
+// The serving loop's hook: admit the next wave (non-blocking) while the grid
+// resolves the current one.
 struct AdmitNext {
   static constexpr bool kActive = true;
   const TableView* t;
@@ -761,45 +730,7 @@ struct AdmitNext {
   WaveDesc* out;
   uint64_t head;
   uint64_t in_flight_puts;
-  uint32_t admit_no;
-  __device__ void operator()() const {
-    serve_admit(*t, *j, out, head, false, in_flight_puts);
-    if ((threadIdx.x & 31) == 0) {
-      __threadfence();
-      atomicExch(j->admit_seq, admit_no);
-    }
-  }
-  // Every thread of every block; block-uniform control flow.
-  __device__ void prefetch() const {
-    __shared__ int s_ok;
-    __shared__ uint32_t s_base;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int ok = 1;
-      for (uint32_t it = 0; ld_acquire_u32(j->admit_seq) != admit_no; ++it) {
-        if (it > kBarrierPolls || (*(volatile uint32_t*)t->status & kStatusBarrier)) {
-          raise_status(t->status, kStatusBarrier);
-          ok = 0;
-          break;
-        }
-        if (it > 256) __nanosleep(64);
-      }
-      s_ok = ok;
-    }
-    __syncthreads();
-    if (!s_ok) return;  // block-uniform; the loop ends at its next barrier
-    const uint32_t n = ld_cg_u32(&out->nops);
-    const uint64_t pos = ld_cg_u64(&out->op_off) % j->arena_cap;
-    const uint32_t set = admit_no & 1u;
-    for (;;) {
-      if (threadIdx.x == 0) s_base = atomicAdd(j->pf_cursor, blockDim.x);
-      __syncthreads();
-      const uint32_t c0 = s_base;
-      __syncthreads();  // s_base is rewritten next round
-      if (c0 >= n) break;  // block-uniform
-      if (c0 + threadIdx.x < n) gather_op(*j, set, pos, c0 + threadIdx.x);
-    }
-  }
+  __device__ void operator()() const { serve_admit(*t, *j, out, head, false, in_flight_puts); }
 };
 
 template <int P>
@@ -823,9 +754,6 @@ __global__ void __launch_bounds__(1024, 1)
   // Admission `a` writes descriptor a & 1, which every block finished
   // reading before the barrier of admission a - 1.
   uint32_t a = 0;
-  // pf: this wave's ops are already in its working-copy set (copied during
-  // the previous wave by the hook's second part); grid-uniform
-  bool pf = false;
   // Barriers behind a blocking admission wait until the admission's own
   // deadline (idle_ns from about now) plus a margin, on the same clock.
   constexpr uint64_t kAdmitMarginNs = 2000000000ull;
@@ -846,37 +774,36 @@ __global__ void __launch_bounds__(1024, 1)
       if (tid == 0) raise_status(t.status, kStatusScratch);
       break;  // grid-uniform (every block read the same descriptor)
     }
-    const uint32_t set = a & 1;  // the working-copy set of this descriptor
     if (nops) {
-      // the wave's ops (contiguous in one lap of the arena) into HBM, unless
-      // the previous wave copied them already
+      // the wave's ops (contiguous in one lap of the arena) into HBM; .cv
+      // loads because the host rewrites arena slots between waves
       const uint64_t pos = op_off % j.arena_cap;
-      if (!pf) {
-        for (uint32_t i = tid; i < nops; i += nt) gather_op(j, set, pos, i);
-        if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+      for (uint32_t i = tid; i < nops; i += nt) {
+        // all three loads before any store: they cross PCIe together
+        const uint8_t ty = __ldcv(j.a_types + pos + i);
+        const uint64_t key = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos + i);
+        const uint64_t val = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos + i);
+        j.d_types[i] = ty;
+        j.d_keys[i] = key;
+        j.d_vals[i] = val;
       }
+      if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
       FusedJob<MapTraits> fj = j.fj;
-      fj.base.types = j.d_types + (size_t)set * j.max_wave_ops;
-      fj.base.keys = j.d_keys + (size_t)set * j.max_wave_ops;
-      fj.base.vals = j.d_vals + (size_t)set * j.max_wave_ops;
+      fj.base.types = j.d_types;
+      fj.base.keys = j.d_keys;
+      fj.base.vals = j.d_vals;
       fj.base.out = j.a_out + pos;  // results go straight to the host-mapped arena
       fj.base.n = nops;
-      // the next wave is admitted by warp 0 during this one's ordering or
-      // resolve step, and its ops are copied into the other set
-      const AdmitNext hook{&t, &j, &j.wave[(a + 1) & 1], first + nreq, wave_puts, a + 1};
-      bool in_sort = false;
-      fused_windows<MapTraits, P, false>(t, sc, fj, bar, smem, seq, hook, &in_sort);
-      if (!in_sort) hook.prefetch();
+      // the next wave is admitted by warp 0 while the others resolve this one
+      fused_windows<MapTraits, P, false>(
+          t, sc, fj, bar, smem, seq,
+          AdmitNext{&t, &j, &j.wave[(a + 1) & 1], first + nreq, wave_puts});
     }
     const uint64_t next = first + nreq;
     ++a;
     if (tid < 32 && nops == 0) serve_admit(t, j, &j.wave[a & 1], next, false, wave_puts);
     if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
-    // the admitted wave's ops were copied iff it has ops (both parts of the
-    // hook ran for every wave with ops); the same value in every thread
-    pf = nops != 0 && ld_cg_u32(&j.wave[a & 1].nops) != 0;
     if (tid == 0) {
-      *j.pf_cursor = 0;  // the next prefetch's claims start after the next barrier
       win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
       __threadfence_system();          // results before the completion count
       ++waves;  // kept in registers: a read of host memory costs a PCIe round trip
@@ -888,7 +815,6 @@ __global__ void __launch_bounds__(1024, 1)
     if (ld_cg_u32(&j.wave[a & 1].nreq) == 0 && ld_cg_u32(&j.wave[a & 1].stop) == 0) {
       // the queue was empty: wait for requests now that wave k is published
       ++a;
-      pf = false;
       if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, true, 0);
       if (!grid_barrier_until(bar, gridDim.x, t.status, seq,
                               global_ns() + j.idle_ns + kAdmitMarginNs))
@@ -2132,10 +2058,10 @@ int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out)
       cudaHostAlloc((void**)&s->a_keys, 8 * arena, fl) == cudaSuccess &&
       cudaHostAlloc((void**)&s->a_vals, 8 * arena, fl) == cudaSuccess &&
       cudaHostAlloc((void**)&s->a_out, sizeof(lsb_result) * arena, fl) == cudaSuccess &&
-      cudaMalloc(&s->d_types, 2ull * wave) == cudaSuccess &&
-      cudaMalloc(&s->d_keys, 16ull * wave) == cudaSuccess &&
-      cudaMalloc(&s->d_vals, 16ull * wave) == cudaSuccess &&
-      cudaMalloc(&s->d_wave, 2 * sizeof(WaveDesc) + 2 * sizeof(uint32_t)) == cudaSuccess &&
+      cudaMalloc(&s->d_types, wave) == cudaSuccess &&
+      cudaMalloc(&s->d_keys, 8ull * wave) == cudaSuccess &&
+      cudaMalloc(&s->d_vals, 8ull * wave) == cudaSuccess &&
+      cudaMalloc(&s->d_wave, 2 * sizeof(WaveDesc)) == cudaSuccess &&
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
   cudaSetDevice(prev);
   if (!ok) {
@@ -2173,8 +2099,6 @@ int lsb_serve_start(lsb_server* s) {
   j.d_keys = s->d_keys;
   j.d_vals = s->d_vals;
   j.wave = s->d_wave;
-  j.admit_seq = reinterpret_cast<uint32_t*>(s->d_wave + 2);
-  j.pf_cursor = j.admit_seq + 1;
   j.max_wave_ops = s->max_wave_ops;
   j.idle_ns = s->idle_ns;
   if (!j.ctl || !j.ring || !j.a_types || !j.a_keys || !j.a_vals || !j.a_out) {
@@ -2214,12 +2138,6 @@ int lsb_serve_start(lsb_server* s) {
   Scratch scv = tb.sc;
   GridBarrier* b = tb.bar;
   void* args[] = {&tv, &scv, &j, &b};
-  // the hook's admission counter and prefetch cursor start at zero
-  if (cudaMemsetAsync(j.admit_seq, 0, 2 * sizeof(uint32_t), s->stream) != cudaSuccess) {
-    cudaGetLastError();
-    cudaSetDevice(prev);
-    return LSB_ERR_CUDA;
-  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(per_sm * tb.num_sms);
   cfg.blockDim = dim3(tb.tune.block);

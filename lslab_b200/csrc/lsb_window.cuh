@@ -1016,19 +1016,14 @@ __device__ void sort_group_warp(const Scratch& sc, const Window<Tr>& w, uint32_t
 // path); then warps take the groups of the big list by a static stride that
 // starts at the warps of blocks without a large group.  No work is claimed
 // through a shared counter, so no grid-wide atomic serializes the phase.
-// `smem` holds kSortSmemBytes.  skip0: block 0 takes no work (its warp 0
-// runs the serving loop's admission meanwhile).
+// `smem` holds kSortSmemBytes.
 template <class Tr>
-__device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t* smem,
-                               bool skip0 = false) {
+__device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t* smem) {
   __shared__ uint32_t s_off;
   const uint32_t tid = threadIdx.x;
-  const uint32_t b0 = skip0 ? 1u : 0u;
-  if (blockIdx.x < b0 || gridDim.x <= b0) return;  // block-uniform
-  const uint32_t bid = blockIdx.x - b0, nb = gridDim.x - b0;
   const bool upd = ld_cg_u32(&w.cnt->upd_count) != 0;  // settled: the probe has ended
   const uint32_t nlarge = ld_cg_u32(&w.cnt->large_count);
-  for (uint32_t job = bid; job < nlarge; job += nb) {
+  for (uint32_t job = blockIdx.x; job < nlarge; job += gridDim.x) {
     const uint32_t gslot = ld_cg_u32(&sc.large[job]) & sc.gmask;
     const uint32_t c = min(g_count(ld_relaxed_u64(&sc.gtab[gslot])), w.n);
     if (c > kHugeMin) continue;  // the huge_* steps order it (c is block-uniform)
@@ -1042,9 +1037,9 @@ __device__ void phase_sort_big(const Scratch& sc, const Window<Tr>& w, uint32_t*
   }
   const uint32_t nbig = ld_cg_u32(&w.cnt->big_count);
   const uint32_t lane = lane_id(), wpb = blockDim.x >> 5;
-  const uint32_t nw = nb * wpb;
-  const uint32_t busy = min(nlarge, nb) * wpb;  // warps of blocks with a large group
-  const uint32_t gw = bid * wpb + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * wpb;
+  const uint32_t busy = min(nlarge, gridDim.x) * wpb;  // warps of blocks with a large group
+  const uint32_t gw = blockIdx.x * wpb + (threadIdx.x >> 5);
   for (uint32_t job = (gw + nw - busy % nw) % nw; job < nbig; job += nw) {
     const uint32_t gslot = ld_cg_u32(&sc.big[job]) & sc.gmask;
     const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[gslot]));
