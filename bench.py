@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--dedup", type=int, default=-1)
     ap.add_argument("--split", type=int, default=-1, help="fused: percent of reads probed first")
     ap.add_argument("--region", type=int, default=-1, help="fused: probe in table-region order")
+    ap.add_argument("--read-order", type=int, default=-1,
+                    help="read calls: 0 auto, 1 table-region order, 2 op order")
     ap.add_argument("--overlap", type=int, default=-1,
                     help="batched calls: 1 = reads in the lean read kernel beside the mutation "
                          "steps on a second stream")
@@ -242,6 +244,8 @@ def apply_tuning(args, table):
         kw["region_order"] = args.region
     if args.overlap >= 0:
         kw["overlap"] = args.overlap
+    if args.read_order >= 0:
+        kw["read_order"] = args.read_order
     if kw:
         table.set_tuning(**kw)
 
@@ -324,7 +328,8 @@ def run_ours(args, world, rank, local):
     # the batch's net effect is one application, so the plain table applies
     # it once too and the two tables stay identical)
     explicit = (args.block or args.prefetch >= 0 or args.chunk >= 0 or args.dedup >= 0
-                or args.split >= 0 or args.region >= 0 or args.overlap >= 0)
+                or args.split >= 0 or args.region >= 0 or args.overlap >= 0
+                or args.read_order >= 0)
     if not args.no_autotune and not explicit:
         fused.autotune(d_types[0], d_keys[0], d_vals[0], out_f[0])
         g = n_get[0]

@@ -127,6 +127,10 @@ typedef struct lsb_tuning {
                              after both (read-mostly windows of many ops); 0 = per-phase
                              launches on the caller's stream (execute) and the persistent
                              kernel (execute_fused) */
+  uint32_t read_order;    /* the lean read kernel (get / contains calls, the reads of the
+                             two-stream form): 0 = auto (reads taken in table-region order
+                             when the table is larger than L2 and a call has at least 2^16
+                             ops), 1 = always in region order, 2 = in op order */
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */

@@ -63,6 +63,7 @@ class Tuning(C.Structure):
         ("region_order", C.c_uint32),
         ("warp_probe", C.c_uint32),
         ("overlap", C.c_uint32),
+        ("read_order", C.c_uint32),
     ]
 
 

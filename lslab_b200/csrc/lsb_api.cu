@@ -92,6 +92,20 @@ __device__ __forceinline__ uint32_t dev_window_slot(const uint32_t* fused_epoch)
   return f + 1 > kFusedEpochs ? 0u : f;
 }
 
+// A read's result in the caller's layout.
+__device__ __forceinline__ void store_read(void* out, uint32_t out_kind, uint32_t i, bool found,
+                                           uint64_t val) {
+  if (out_kind == kOutResult) {
+    uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
+    st_cs_u64(p, found ? 1ull : 0ull);
+    st_cs_u64(p + 1, found ? val : 0ull);
+  } else if (out_kind == kOutResult32) {
+    st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
+  } else if (out_kind == kOutBool) {
+    st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+  }
+}
+
 // Read-only batch (get / contains) in its lean form: one op per thread, no
 // grouping, no work claims, the result written straight out; with `types`,
 // the reads of a mixed window (other ops are left to the engine).  The code is
@@ -115,15 +129,105 @@ __global__ void __launch_bounds__(256, 8)
       key = (Key)ld_cs_u32(keys + i);
     uint64_t val;
     const bool found = read_lookup<Tr>(t, key, &val);
-    if (out_kind == kOutResult) {
-      uint64_t* p = (uint64_t*)out + 2 * (size_t)i;
-      st_cs_u64(p, found ? 1ull : 0ull);
-      st_cs_u64(p + 1, found ? val : 0ull);
-    } else if (out_kind == kOutResult32) {
-      st_cs_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
-    } else if (out_kind == kOutBool) {
-      st_cs_u8((uint8_t*)out + i, found ? 1 : 0);
+    store_read(out, out_kind, i, found, val);
+  }
+}
+
+// Reads in table-region order.  Over a table larger than L2, a batch's reads
+// taken in the order of their bucket's region (64 equal ranges of the slab
+// array) run ~1.9x faster on Zipf keys (40 -> 21 us for 2^20 gets over 2^22
+// buckets, measured with the batch pre-ordered on the host): the repeats of a
+// hot key and the slabs of a region meet in the same SMs' caches and address
+// translation entries.  Three steps order the reads on the device: block b
+// counts the reads of ops [b * kBinChunk, ...) per region, one block turns
+// the counts into region-major offsets, block b writes its reads' op indices
+// at those offsets; then k_read_ordered reads through the order.
+constexpr uint32_t kReadRegions = 64;
+constexpr uint32_t kBinChunk = 4096;
+
+template <class Tr>
+__device__ __forceinline__ uint32_t read_region(const TableView& t, typename Tr::Key key,
+                                                uint32_t shift) {
+  return ((uint32_t)Tr::hash(key) & t.mask) >> shift;
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(256)
+    k_bin_count(TableView t, const uint8_t* types, const typename Tr::Key* keys, uint32_t n,
+                uint32_t shift, uint32_t* hist) {
+  __shared__ uint32_t h[kReadRegions];
+  if (threadIdx.x < kReadRegions) h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t base = blockIdx.x * kBinChunk, end = min(n, base + kBinChunk);
+  // warp-uniform loop: every lane takes part in the aggregation
+  for (uint32_t i0 = base + (threadIdx.x & ~31u); i0 < end; i0 += blockDim.x) {
+    const uint32_t i = i0 + lane;
+    uint32_t r = kReadRegions;
+    if (i < end && (types == nullptr || types[i] == kOpRead))
+      r = read_region<Tr>(t, keys[i], shift);
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, r);
+    if (r < kReadRegions && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&h[r], __popc(peers));
+  }
+  __syncthreads();
+  if (threadIdx.x < kReadRegions) hist[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+}
+
+// One block: hist (region-major, m entries) becomes exclusive offsets; the
+// total (the read count) goes to hist[m].
+__global__ void __launch_bounds__(1024) k_bin_scan(uint32_t* hist, uint32_t m) {
+  __shared__ uint32_t tmp[32];
+  const uint32_t per = (m + blockDim.x - 1) / blockDim.x, j0 = threadIdx.x * per;
+  uint32_t local = 0;
+  for (uint32_t k = 0; k < per; ++k)
+    if (j0 + k < m) local += hist[j0 + k];
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(local, tmp, &total);
+  for (uint32_t k = 0; k < per; ++k)
+    if (j0 + k < m) {
+      const uint32_t c = hist[j0 + k];
+      hist[j0 + k] = run;
+      run += c;
     }
+  if (threadIdx.x == 0) hist[m] = total;
+}
+
+template <class Tr>
+__global__ void __launch_bounds__(256)
+    k_bin_scatter(TableView t, const uint8_t* types, const typename Tr::Key* keys, uint32_t n,
+                  uint32_t shift, const uint32_t* offs, uint32_t* order) {
+  __shared__ uint32_t cur[kReadRegions];
+  if (threadIdx.x < kReadRegions) cur[threadIdx.x] = offs[threadIdx.x * gridDim.x + blockIdx.x];
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t base = blockIdx.x * kBinChunk, end = min(n, base + kBinChunk);
+  for (uint32_t i0 = base + (threadIdx.x & ~31u); i0 < end; i0 += blockDim.x) {
+    const uint32_t i = i0 + lane;
+    uint32_t r = kReadRegions;
+    if (i < end && (types == nullptr || types[i] == kOpRead))
+      r = read_region<Tr>(t, keys[i], shift);
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, r);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (r < kReadRegions && lane == leader) pos = atomicAdd(&cur[r], __popc(peers));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, leader) + __popc(peers & ((1u << lane) - 1u));
+    if (r < kReadRegions && pos < n) order[pos] = i;
+  }
+}
+
+// The reads through the region order: thread t serves op order[t] for t
+// below the read count (order[n] holds nothing; the count is hist's total).
+template <class Tr>
+__global__ void __launch_bounds__(256, 8)
+    k_read_ordered(TableView t, const uint32_t* order, const uint32_t* count,
+                   const typename Tr::Key* keys, void* out, uint32_t out_kind, uint32_t n) {
+  const uint32_t c = min(ld_cg_u32(count), n);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c; k += gridDim.x * blockDim.x) {
+    const uint32_t i = ld_cs_u32(order + k);
+    if (i >= n) continue;  // read back from scratch: checked before use
+    uint64_t val;
+    const bool found = read_lookup<Tr>(t, (typename Tr::Key)keys[i], &val);
+    store_read(out, out_kind, i, found, val);
   }
 }
 
@@ -896,13 +1000,15 @@ struct Tuning {
   uint32_t dedup = 0;
   uint32_t warp_probe = 0;  // read-only batches through k_read_coop
   uint32_t overlap = 0;     // mixed windows: reads in k_read beside the mutation steps
+  uint32_t read_order = 0;  // 0 auto, 1 table-region order, 2 op order
 };
 
 inline bool tuning_ok(const lsb_tuning& x) {
   return (x.block_threads == 128 || x.block_threads == 256 || x.block_threads == 512 ||
           x.block_threads == 1024) &&
          x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
-         x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1 && x.overlap <= 1;
+         x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1 && x.overlap <= 1 &&
+         x.read_order <= 2;
 }
 
 template <class Tr>
@@ -933,6 +1039,7 @@ struct Table {
   // stream priority, so its blocks take SMs as k_read's blocks retire)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  uint32_t* rhist = nullptr;  // region counts of ordered reads (+ the read count)
 
   TableView view() const {
     TableView v;
@@ -951,7 +1058,7 @@ struct Table {
     void* ptrs[] = {slabs, locks, status, pool, free_stack, sc.gtab, sc.ginl, sc.ctab, sc.cdat,
                     sc.minfo, sc.mloc, sc.pred, sc.goff, sc.seg, sc.mlist, sc.big, sc.large,
                     sc.cnt, sc.obin, sc.perm, sc.clist, sc.hlist, sc.hrec, sc.hbins, sc.hrun, sc.runs,
-                    sc.lnu, sc.rnu, trace, fused_epoch};
+                    sc.lnu, sc.rnu, trace, fused_epoch, rhist};
     for (void* p : ptrs) cudaFree(p);
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -1014,7 +1121,9 @@ struct Table {
         cudaMalloc(&sc.lnu, sizeof(uint32_t) * window) == cudaSuccess &&
         cudaMalloc(&sc.rnu, sizeof(uint32_t) * (size_t)sc.rcap) == cudaSuccess &&
         cudaMalloc(&sc.cnt, kCounterBytes) == cudaSuccess &&
-        cudaMalloc(&fused_epoch, sizeof(uint32_t)) == cudaSuccess;
+        cudaMalloc(&fused_epoch, sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&rhist, sizeof(uint32_t) * ((window / kBinChunk + 1) * (size_t)kReadRegions + 1)) ==
+            cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       return LSB_ERR_OOM;
@@ -1060,6 +1169,7 @@ struct Table {
     tune.dedup = x.dedup;
     tune.warp_probe = x.warp_probe;
     tune.overlap = x.overlap;
+    tune.read_order = x.read_order;
     split_q16 = (uint32_t)(((uint64_t)x.fused_split << 16) / 100);
     binned = x.region_order != 0;
     return LSB_OK;
@@ -1074,6 +1184,7 @@ struct Table {
     x->region_order = binned ? 1u : 0u;
     x->warp_probe = tune.warp_probe;
     x->overlap = tune.overlap;
+    x->read_order = tune.read_order;
   }
 
   // Epoch of the next per-phase window (even: 2, 4, ...; the fused path uses
@@ -1129,8 +1240,41 @@ struct Table {
   // Read-only batch: the lean read kernel (k_read), or, with in-warp dedup
   // or reader locks, the tuned probe kernel (one launch per 2^23 ops, no
   // grouping).
+  // Whether a read call of m ops takes its reads in table-region order.
+  bool ordered_reads(size_t m) const {
+    if (tune.read_order == 2) return false;
+    if (tune.read_order == 1) return true;
+    return (uint64_t)buckets * Tr::kSlabBytes > (128ull << 20) && m >= (1u << 16);
+  }
+
+  // The reads among ops [0, m) (all of them without types) in table-region
+  // order: count, offsets, order, then the lookups (m <= the window size).
+  int launch_read_ordered(const uint8_t* types, const typename Tr::Key* keys, void* out,
+                          uint32_t out_kind, uint32_t m, cudaStream_t s) {
+    if (m == 0) return LSB_OK;
+    if (m > sc.max_window) return LSB_ERR_ARG;
+    const uint32_t shift = log2 > 6 ? log2 - 6 : 0u;
+    const uint32_t nb = (m + kBinChunk - 1) / kBinChunk;
+    k_bin_count<Tr><<<nb, 256, 0, s>>>(view(), types, keys, m, shift, rhist);
+    k_bin_scan<<<1, 1024, 0, s>>>(rhist, nb * kReadRegions);
+    k_bin_scatter<Tr><<<nb, 256, 0, s>>>(view(), types, keys, m, shift, rhist, sc.perm);
+    k_read_ordered<Tr><<<(m + 255) / 256, 256, 0, s>>>(view(), sc.perm, rhist + nb * kReadRegions,
+                                                       keys, out, out_kind, m);
+    LSB_CK(cudaGetLastError());
+    return LSB_OK;
+  }
+
   int run_reads(const typename Tr::Key* keys, void* out, uint32_t out_kind, size_t n,
                 cudaStream_t s) {
+    if (!tune.dedup && lock_mode != kLockRW && !tune.warp_probe && ordered_reads(n)) {
+      for (size_t off = 0; off < n; off += sc.max_window) {
+        const uint32_t m = (uint32_t)std::min<size_t>(sc.max_window, n - off);
+        void* o = out ? (uint8_t*)out + off * out_elem(out_kind) : nullptr;
+        int e = launch_read_ordered(nullptr, keys + off, o, out ? out_kind : kOutNone, m, s);
+        if (e) return e;
+      }
+      return LSB_OK;
+    }
     if (!tune.dedup && lock_mode != kLockRW) {
       for (size_t off = 0; off < n; off += (size_t)1 << 30) {
         const uint32_t m = (uint32_t)std::min<size_t>((size_t)1 << 30, n - off);
@@ -1220,12 +1364,16 @@ struct Table {
           LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_mutations<Tr>, args));
         }
         LSB_CK(cudaEventRecord(ev_join, side));
-        const uint32_t rblocks = LSB_OVERLAP_READ_BLOCKS
-                                     ? std::min<uint32_t>((m + 255) / 256,
-                                                          num_sms * LSB_OVERLAP_READ_BLOCKS)
-                                     : (m + 255) / 256;
-        k_read<Tr><<<std::max(1u, rblocks), 256, 0, s>>>(view(), w.types, w.keys, w.out,
-                                                          w.out_kind, m);
+        if (ordered_reads(m)) {
+          if (int e2 = launch_read_ordered(w.types, w.keys, w.out, w.out_kind, m, s)) return e2;
+        } else {
+          const uint32_t rblocks = LSB_OVERLAP_READ_BLOCKS
+                                       ? std::min<uint32_t>((m + 255) / 256,
+                                                            num_sms * LSB_OVERLAP_READ_BLOCKS)
+                                       : (m + 255) / 256;
+          k_read<Tr><<<std::max(1u, rblocks), 256, 0, s>>>(view(), w.types, w.keys, w.out,
+                                                            w.out_kind, m);
+        }
         LSB_CK(cudaStreamWaitEvent(s, ev_join, 0));
       } else {
         launch_probe<true>(grid_for(m), w, s);
