@@ -95,7 +95,7 @@ def parse():
     ap.add_argument("--split", type=int, default=-1, help="fused: percent of reads probed first")
     ap.add_argument("--region", type=int, default=-1, help="fused: probe in table-region order")
     ap.add_argument("--read-order", type=int, default=-1,
-                    help="read calls: 0 auto, 1 table-region order, 2 op order")
+                    help="read calls: 0 op order, 1 table-region order")
     ap.add_argument("--overlap", type=int, default=-1,
                     help="batched calls: 1 = reads in the lean read kernel beside the mutation "
                          "steps on a second stream")

@@ -128,9 +128,9 @@ typedef struct lsb_tuning {
                              launches on the caller's stream (execute) and the persistent
                              kernel (execute_fused) */
   uint32_t read_order;    /* the lean read kernel (get / contains calls, the reads of the
-                             two-stream form): 0 = auto (reads taken in table-region order
-                             when the table is larger than L2 and a call has at least 2^16
-                             ops), 1 = always in region order, 2 = in op order */
+                             two-stream form): 0 = in op order (default), 1 = in table-region
+                             order built on the device first (measured slower: the ordering
+                             steps cost more than the locality saves) */
 } lsb_tuning;
 
 #define LSB_LOCK_WRITER 0u   /* writers take a per-bucket lock; readers never lock   */

@@ -133,15 +133,32 @@ __global__ void __launch_bounds__(256, 8)
   }
 }
 
-// Reads in table-region order.  Over a table larger than L2, a batch's reads
-// taken in the order of their bucket's region (64 equal ranges of the slab
-// array) run ~1.9x faster on Zipf keys (40 -> 21 us for 2^20 gets over 2^22
-// buckets, measured with the batch pre-ordered on the host): the repeats of a
-// hot key and the slabs of a region meet in the same SMs' caches and address
-// translation entries.  Three steps order the reads on the device: block b
-// counts the reads of ops [b * kBinChunk, ...) per region, one block turns
-// the counts into region-major offsets, block b writes its reads' op indices
-// at those offsets; then k_read_ordered reads through the order.
+// A read's result written out of op order: one 16-byte store cached in L2
+// (results land scattered over the output, so streaming half-sector stores
+// would make L2 fetch the rest of each sector).
+__device__ __forceinline__ void store_read_scattered(void* out, uint32_t out_kind, uint32_t i,
+                                                     bool found, uint64_t val) {
+  if (out_kind == kOutResult)
+    st_cg_v2u64((uint64_t*)out + 2 * (size_t)i, found ? 1ull : 0ull, found ? val : 0ull);
+  else if (out_kind == kOutResult32)
+    st_cg_u64((uint64_t*)out + i, found ? (1ull | (val << 32)) : 0ull);
+  else if (out_kind == kOutBool)
+    st_cg_u8((uint8_t*)out + i, found ? 1 : 0);
+}
+
+// Reads in table-region order (tuning read_order 1).  Over a table larger
+// than L2, a batch's reads taken in the order of their bucket's region (64
+// equal ranges of the slab array) run ~1.9x faster on Zipf keys when the
+// batch arrives ordered (40 -> 21 us for 2^20 gets over 2^22 buckets): the
+// repeats of a hot key and the slabs of a region meet in the same SMs'
+// caches and address-translation entries.  Built on the device the order
+// does not pay (measured per kernel: count 15, offsets 19, scatter 20, reads
+// through the order 29 us, against 38-40 us for the reads in op order, the
+// ordered reads slowed by the key gather and the scattered result stores),
+// so it is off by default.  Three steps order the reads: block b counts the
+// reads of ops [b * kBinChunk, ...) per region, one block turns the counts
+// into region-major offsets, block b writes its reads' op indices at those
+// offsets; then k_read_ordered reads through the order.
 constexpr uint32_t kReadRegions = 64;
 constexpr uint32_t kBinChunk = 4096;
 
@@ -227,7 +244,7 @@ __global__ void __launch_bounds__(256, 8)
     if (i >= n) continue;  // read back from scratch: checked before use
     uint64_t val;
     const bool found = read_lookup<Tr>(t, (typename Tr::Key)keys[i], &val);
-    store_read(out, out_kind, i, found, val);
+    store_read_scattered(out, out_kind, i, found, val);
   }
 }
 
@@ -1000,7 +1017,7 @@ struct Tuning {
   uint32_t dedup = 0;
   uint32_t warp_probe = 0;  // read-only batches through k_read_coop
   uint32_t overlap = 0;     // mixed windows: reads in k_read beside the mutation steps
-  uint32_t read_order = 0;  // 0 auto, 1 table-region order, 2 op order
+  uint32_t read_order = 0;  // 1: read calls in table-region order (slower; measured)
 };
 
 inline bool tuning_ok(const lsb_tuning& x) {
@@ -1008,7 +1025,7 @@ inline bool tuning_ok(const lsb_tuning& x) {
           x.block_threads == 1024) &&
          x.prefetch <= 2 && x.dedup <= 1 && x.chunk % 32 == 0 && x.chunk <= (1u << 20) &&
          x.fused_split <= 100 && x.region_order <= 1 && x.warp_probe <= 1 && x.overlap <= 1 &&
-         x.read_order <= 2;
+         x.read_order <= 1;
 }
 
 template <class Tr>
@@ -1240,12 +1257,8 @@ struct Table {
   // Read-only batch: the lean read kernel (k_read), or, with in-warp dedup
   // or reader locks, the tuned probe kernel (one launch per 2^23 ops, no
   // grouping).
-  // Whether a read call of m ops takes its reads in table-region order.
-  bool ordered_reads(size_t m) const {
-    if (tune.read_order == 2) return false;
-    if (tune.read_order == 1) return true;
-    return (uint64_t)buckets * Tr::kSlabBytes > (128ull << 20) && m >= (1u << 16);
-  }
+  // Whether a read call takes its reads in table-region order.
+  bool ordered_reads(size_t) const { return tune.read_order == 1; }
 
   // The reads among ops [0, m) (all of them without types) in table-region
   // order: count, offsets, order, then the lookups (m <= the window size).
