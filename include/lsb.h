@@ -222,7 +222,13 @@ int lsb_map_set_tuning(lsb_map* m, const lsb_tuning* t);
  * one %globaltimer stamp per phase boundary per window: entry = ns << 8 |
  * (window & 63) << 2 | phase, phase 0 window start, 1 probe done, 2 ordering
  * done, 3 resolve done.  read_trace copies the last launch's entries to host
- * memory (synchronises the stream). */
+ * memory (synchronises the stream).  When the last call ran two-stream
+ * windows (tuning overlap), the entries come from timing events instead, ns
+ * counted from the first window's start, for each window (< 16, window field
+ * = window & 31): phase 0 start, 1 read kernel done, 2 mutation steps
+ * (listing, probing, ordering) done, 3 resolve done, and with window field
+ * | 32: phase 1 listing done, phase 2 probing done.  Calls issued while the
+ * stream is being captured record none. */
 int lsb_map_set_trace(lsb_map* m, int on);
 int lsb_map_read_trace(lsb_map* m, uint64_t* out, size_t cap, size_t* count,
                        cudaStream_t stream);

@@ -69,6 +69,12 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_OVERLAP_READ_BLOCKS
 #define LSB_OVERLAP_READ_BLOCKS 0
 #endif
+// LSB_OVERLAP_READ_WAIT 1: the read kernel starts once the mutation list is
+// built, so the probe-and-group kernel (higher stream priority) takes its
+// blocks before the reads fill the SMs; 0: the reads start with the window.
+#ifndef LSB_OVERLAP_READ_WAIT
+#define LSB_OVERLAP_READ_WAIT 0
+#endif
 // two read lookups in flight per thread in the fused kernel's lean read
 // loop: measured slower at the 64-register cap (more spills), so off
 #ifndef LSB_FUSED_READ_PAIR
@@ -79,7 +85,8 @@ __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
   const uint32_t warp = spread_warp();
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
+  phase_probe<Tr, kGroup, P, P == 1>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk,
+                                     dedup != 0);
 }
 
 // Windows run as launches on two streams (Table::run_plain, tuning overlap)
@@ -365,7 +372,7 @@ template <class Tr>
 __global__ void __launch_bounds__(256, 4)
     k_probe_list(TableView t, Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
   w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
-  phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
+  phase_probe_list<Tr, true>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
 }
 
 // The mutation steps of a window whose reads run beside it in k_read (the
@@ -392,7 +399,7 @@ __global__ void __launch_bounds__(256, 4)
   }
   phase_list_muts<Tr>(sc, w, warp, nwarps);
   if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
-  phase_probe_list<Tr>(t, sc, w, warp, nwarps, false);
+  phase_probe_list<Tr, true>(t, sc, w, warp, nwarps, false);
   if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe step has ended
@@ -1052,11 +1059,19 @@ struct Table {
   uint32_t* fused_epoch = nullptr;  // device counter of fused windows (see k_fused)
   bool binned = false;         // fused path probes in table-region order (measured slower)
   int fused_per_sm[3][4] = {};  // occupancy by (prefetch, block size) once queried
+  int resolve_per_sm = 0;       // resident 256-thread k_resolve blocks per SM once queried
   // tuning overlap: the mutation steps of a window run on `side` (highest
   // stream priority, so its blocks take SMs as k_read's blocks retire)
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_list = nullptr;
   uint32_t* rhist = nullptr;  // region counts of ordered reads (+ the read count)
+  // Tracing of the two-stream form: per window, timing events at its start
+  // and after each of its kernels (kSpanPoints points, kSpanWindows windows
+  // of the last call), read back by read_trace.
+  static constexpr int kSpanPoints = 6;  // start, list, probe, ordering, reads, resolve
+  static constexpr int kSpanWindows = 16;
+  cudaEvent_t span_ev[kSpanWindows][kSpanPoints] = {};
+  int span_windows = 0;  // windows of the last traced two-stream call (0: none)
 
   TableView view() const {
     TableView v;
@@ -1080,6 +1095,32 @@ struct Table {
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_list) cudaEventDestroy(ev_list);
+    destroy_spans();
+  }
+
+  void destroy_spans() {
+    for (auto& w : span_ev)
+      for (auto& e : w)
+        if (e) {
+          cudaEventDestroy(e);
+          e = nullptr;
+        }
+    span_windows = 0;
+  }
+
+  // Timing event `point` of two-stream window `wi` on stream `st`, when
+  // tracing is on and the stream is not being captured.
+  int span_mark(int wi, int point, cudaStream_t st) {
+    if (!trace || wi >= kSpanWindows) return LSB_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LSB_CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return LSB_OK;
+    cudaEvent_t& e = span_ev[wi][point];
+    if (!e) LSB_CK(cudaEventCreate(&e));
+    LSB_CK(cudaEventRecord(e, st));
+    if (point == 0) span_windows = wi + 1;
+    return LSB_OK;
   }
 
   int init(unsigned log2_buckets, const lsb_options* opt) {
@@ -1175,6 +1216,7 @@ struct Table {
     LSB_CK(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
     LSB_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     LSB_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    LSB_CK(cudaEventCreateWithFlags(&ev_list, cudaEventDisableTiming));
     return LSB_OK;
   }
 
@@ -1343,7 +1385,10 @@ struct Table {
       // the counters and the sort launch's grid barrier are zero here: the
       // previous launch's last block cleared them (release_counters)
       uint32_t* dev_epoch = overlap ? fused_epoch : nullptr;
+      const int wi = (int)(off / W);
+      if (overlap && off == 0) span_windows = 0;
       if (overlap) {
+        if (int e2 = span_mark(wi, 0, s)) return e2;
         // Reads write their results at probe time and never join a group;
         // only reads after a same-key mutation are rewritten by the resolve
         // step, which is also the only step that writes the table.  So the
@@ -1357,7 +1402,13 @@ struct Table {
           const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
           k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256,
                             0, side>>>(sc, w, fused_epoch);
+          if (int e2 = span_mark(wi, 1, side)) return e2;
+          if (LSB_OVERLAP_READ_WAIT) {
+            LSB_CK(cudaEventRecord(ev_list, side));
+            LSB_CK(cudaStreamWaitEvent(s, ev_list, 0));
+          }
           k_probe_list<Tr><<<num_sms * 2, 256, 0, side>>>(view(), sc, w, fused_epoch);
+          if (int e2 = span_mark(wi, 2, side)) return e2;
           if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
         } else {
           TableView tv = view();
@@ -1376,6 +1427,7 @@ struct Table {
           cfg.numAttrs = 1;
           LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_mutations<Tr>, args));
         }
+        if (int e2 = span_mark(wi, 3, side)) return e2;
         LSB_CK(cudaEventRecord(ev_join, side));
         if (ordered_reads(m)) {
           if (int e2 = launch_read_ordered(w.types, w.keys, w.out, w.out_kind, m, s)) return e2;
@@ -1387,14 +1439,27 @@ struct Table {
           k_read<Tr><<<std::max(1u, rblocks), 256, 0, s>>>(view(), w.types, w.keys, w.out,
                                                             w.out_kind, m);
         }
+        if (int e2 = span_mark(wi, 4, s)) return e2;
         LSB_CK(cudaStreamWaitEvent(s, ev_join, 0));
       } else {
         launch_probe<true>(grid_for(m), w, s);
         if (int e2 = launch_sort(w, s, nullptr)) return e2;
       }
-      const int rgrid = std::max(1, std::min<int>(num_sms * 8, (int)((m + 255) / 256)));
+      // One wave of blocks at most: the step's work is the window's
+      // mutations (and the reads after its first one), walked by a grid
+      // stride, and a second wave would run the same dependent chain again
+      // after the first (20 against 10 us for the 52k puts of a 2^20-op
+      // 95/5 window with a grid of one thread per op).
+      if (resolve_per_sm == 0 &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, k_resolve<Tr>, 256, 0) !=
+              cudaSuccess)
+        resolve_per_sm = 4;
+      const int rgrid =
+          std::max(1, std::min<int>(num_sms * std::max(1, resolve_per_sm), (int)((m + 255) / 256)));
       k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar, dev_epoch);
       LSB_CK(cudaGetLastError());
+      if (overlap)
+        if (int e2 = span_mark(wi, 5, s)) return e2;
     }
     return LSB_OK;
   }
@@ -1439,6 +1504,7 @@ struct Table {
     // windows as launches on two streams (reads beside the mutation steps)
     if (tune.overlap && types != nullptr && !tune.dedup && lock_mode != kLockRW)
       return run_plain(types, uniform, keys, 1, vals, 1, out, out_kind, n, s);
+    span_windows = 0;  // read_trace reports this launch's phase stamps
     FusedJob<Tr> job;
     job.base = window(types, uniform, keys, 1, vals, 1, out, out_kind, (uint32_t)n);
     job.window = sc.max_window;
@@ -1492,6 +1558,27 @@ struct Table {
     if (!trace) return LSB_ERR_STATE;
     std::vector<uint64_t> h(kTraceCap);
     LSB_CK(cudaStreamSynchronize(s));
+    if (span_windows > 0) {
+      // the last call ran two-stream windows: entries from their events,
+      // ns counted from the first window's start (+1 us, so none is zero)
+      LSB_CK(cudaStreamSynchronize(side));
+      static const uint32_t kPhase[kSpanPoints] = {0, 1, 2, 2, 1, 3};
+      static const uint32_t kSub[kSpanPoints] = {0, 0x20, 0x20, 0, 0, 0};
+      size_t n = 0;
+      for (int wi = 0; wi < span_windows; ++wi)
+        for (int p = 0; p < kSpanPoints; ++p) {
+          if (!span_ev[wi][p]) continue;
+          float ms = 0.f;
+          LSB_CK(cudaEventElapsedTime(&ms, span_ev[0][0], span_ev[wi][p]));
+          const uint64_t ns = 1000ull + (uint64_t)(ms * 1e6f);
+          const uint64_t e =
+              (ns << 8) | ((uint64_t)(((uint32_t)wi & 0x1Fu) | kSub[p]) << 2) | kPhase[p];
+          if (n < cap) out[n] = e;
+          ++n;
+        }
+      if (count) *count = n;
+      return LSB_OK;
+    }
     LSB_CK(cudaMemcpy(h.data(), trace, sizeof(uint64_t) * kTraceCap, cudaMemcpyDeviceToHost));
     size_t n = 0;
     while (n < kTraceCap && h[n] != 0) ++n;
