@@ -75,6 +75,11 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_OVERLAP_READ_WAIT
 #define LSB_OVERLAP_READ_WAIT 0
 #endif
+// threads per block of the ordering kernel k_sort (one block per SM; a
+// block orders one big group at a time)
+#ifndef LSB_SORT_THREADS
+#define LSB_SORT_THREADS 256
+#endif
 // two read lookups in flight per thread in the fused kernel's lean read
 // loop: measured slower at the 64-register cap (more spills), so off
 #ifndef LSB_FUSED_READ_PAIR
@@ -85,8 +90,7 @@ __global__ void __launch_bounds__(1024, LSB_PROBE_MIN_BLOCKS)
     k_probe(TableView t, Scratch sc, Window<Tr> w, uint32_t chunk, uint32_t dedup) {
   const uint32_t warp = spread_warp();
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  phase_probe<Tr, kGroup, P, P == 1>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk,
-                                     dedup != 0);
+  phase_probe<Tr, kGroup, P>(t, sc, w, warp, nwarps, &w.cnt->probe_cursor, chunk, dedup != 0);
 }
 
 // Windows run as launches on two streams (Table::run_plain, tuning overlap)
@@ -372,7 +376,7 @@ template <class Tr>
 __global__ void __launch_bounds__(256, 4)
     k_probe_list(TableView t, Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
   w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
-  phase_probe_list<Tr, true>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
+  phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
 }
 
 // The mutation steps of a window whose reads run beside it in k_read (the
@@ -399,7 +403,7 @@ __global__ void __launch_bounds__(256, 4)
   }
   phase_list_muts<Tr>(sc, w, warp, nwarps);
   if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
-  phase_probe_list<Tr, true>(t, sc, w, warp, nwarps, false);
+  phase_probe_list<Tr>(t, sc, w, warp, nwarps, false);
   if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe step has ended
@@ -1471,7 +1475,7 @@ struct Table {
     void* args[] = {&sc, &w, &b, &dev_epoch};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(num_sms);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(LSB_SORT_THREADS);
     cfg.dynamicSmemBytes = kSortSmemBytes;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];

@@ -12,9 +12,6 @@
 // Tag byte: 0x00 empty (never used), 0x80 busy (being claimed), 0x80|fp live,
 // fp dead (removed; key kept so a later insert of the same key revives it).
 // fp in 1..127 comes from the high half of the hash; the bucket from the low.
-// A key's home group (home_group) is a pair of map slots or a quad of set
-// slots in its head slab that inserts fill first, so that lookups can load
-// it beside the meta sector.
 //
 // Reference counterparts: slab_node/set_node (include/lslab/detail/slab_node.h:13-35:
 // 31 keys + valid bitmap + next in lane 31's slot, values in a second array),
@@ -69,19 +66,6 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t k) {
 
 __device__ __forceinline__ uint32_t fingerprint(uint64_t h) {
   return 1u + (uint32_t)(((h >> 32) * 127ull) >> 32);  // 1..127
-}
-
-// Home group of a key in its bucket's head slab: kHomeSlots consecutive
-// slots (map: a pair, one 32-B sector; set: a quad, 16 B) that an insert
-// takes first when one of them is free (scan_chain), so that a lookup can
-// load the group's keys together with the meta sector rather than after it
-// (read_lookup, table_find_n): one round trip to memory instead of two for
-// most hits.  Placement never changes results, only how fast a key is found.
-// From bits 32..55 of the hash (the bucket takes the low bits, the
-// fingerprint is set by the top ones).
-template <class Tr>
-__device__ __forceinline__ uint32_t home_group(uint64_t h) {
-  return (((uint32_t)(h >> 32) & 0xFFFFFFu) * Tr::kHomeGroups) >> 24;
 }
 
 // ------------------------------------------------------------- memory ops
@@ -153,12 +137,6 @@ __device__ __forceinline__ ulonglong2 ld_ca_v2u64(const void* p) {
 __device__ __forceinline__ uint32_t ld_ca_u32(const void* p) {
   uint32_t r;
   asm volatile("ld.global.ca.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(l2_keep()));
-  return r;
-}
-
-__device__ __forceinline__ uint64_t ld_ca_u64(const void* p) {
-  uint64_t r;
-  asm volatile("ld.global.ca.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(r) : "l"(p), "l"(l2_keep()));
   return r;
 }
 
@@ -308,8 +286,6 @@ struct MapTraits {
   // its own key: a reader that matched the old key could otherwise read the
   // new key's value.  Locked inserts reuse any dead slot (scan_chain).
   static constexpr bool kReuseDead = false;
-  static constexpr uint32_t kHomeSlots = 2;    // one 32-B sector of two slots
-  static constexpr uint32_t kHomeGroups = 14;  // 28 slots
   __device__ static uint64_t hash(Key k) { return mix64(k); }
 };
 
@@ -321,8 +297,6 @@ struct SetTraits {
   // Without values a reader only ever compares the key itself, so any dead
   // slot can take a new key.
   static constexpr bool kReuseDead = true;
-  static constexpr uint32_t kHomeSlots = 4;   // one 16-B quad of keys
-  static constexpr uint32_t kHomeGroups = 7;  // 28 slots
   __device__ static uint64_t hash(Key k) { return mix64((uint64_t)k); }
 };
 
@@ -450,49 +424,6 @@ constexpr uint64_t kLocLive = 1ull << 63;
 __device__ __forceinline__ uint32_t loc_slab(uint64_t loc) { return (uint32_t)(loc >> 8); }
 __device__ __forceinline__ int loc_slot(uint64_t loc) { return (int)(loc & 0xFFu); }
 
-// The keys of a head slab's home group, loaded beside its meta sector.
-template <class Tr>
-struct HomeKeys;
-template <>
-struct HomeKeys<MapTraits> {
-  uint64_t k0, k1;
-};
-template <>
-struct HomeKeys<SetTraits> {
-  uint4 k;
-};
-
-template <class Tr>
-__device__ __forceinline__ HomeKeys<Tr> load_home(const uint8_t* slab, uint32_t g) {
-  const uint8_t* p = slab + kMetaBytes + g * Tr::kHomeSlots * Tr::kSlotBytes;
-  HomeKeys<Tr> hk;
-  if constexpr (Tr::kHasValue) {
-    hk.k0 = ld_ca_u64(p);
-    hk.k1 = ld_ca_u64(p + Tr::kSlotBytes);
-  } else {
-    hk.k = ld_ca_v4(p);
-  }
-  return hk;
-}
-
-// Slot of `key` in its home group (live tags in `hbits`, bit j = slot j of
-// the group), or -1.
-template <class Tr>
-__device__ __forceinline__ int home_slot(const HomeKeys<Tr>& hk, uint32_t hbits,
-                                         typename Tr::Key key) {
-  if constexpr (Tr::kHasValue) {
-    if ((hbits & 1u) && hk.k0 == (uint64_t)key) return 0;
-    if ((hbits & 2u) && hk.k1 == (uint64_t)key) return 1;
-  } else {
-    const uint32_t k = (uint32_t)key;
-    if ((hbits & 1u) && hk.k.x == k) return 0;
-    if ((hbits & 2u) && hk.k.y == k) return 1;
-    if ((hbits & 4u) && hk.k.z == k) return 2;
-    if ((hbits & 8u) && hk.k.w == k) return 3;
-  }
-  return -1;
-}
-
 // Continue a lookup in slab `s`, trying its candidate slots `cand`, then
 // the chain from `next` (s's link).  Takes the link rather than the whole
 // meta sector so that callers need not keep the tag words live.
@@ -542,10 +473,7 @@ __device__ __forceinline__ bool table_find(const TableView& t, typename Tr::Key 
 // kernel's read loop): the head meta sector, the first candidate slot inline,
 // the rest of the chain in find_rest.  Few registers: it runs in kernels
 // bounded to 32 a thread.
-#ifndef LSB_READ_HOME
-#define LSB_READ_HOME 1
-#endif
-template <class Tr, bool kHome = LSB_READ_HOME != 0>
+template <class Tr>
 __device__ __forceinline__ bool read_lookup(const TableView& t, typename Tr::Key key,
                                             uint64_t* val) {
   const uint64_t h = Tr::hash(key);
@@ -553,26 +481,8 @@ __device__ __forceinline__ bool read_lookup(const TableView& t, typename Tr::Key
   const uint32_t rep = (0x80u | fingerprint(h)) * 0x01010101u;
   const uint8_t* slab = slab_ptr((const uint8_t*)t.slabs, s, Tr::kSlabBytes);
   const Meta m = load_meta<true>(slab);
-  uint32_t cand;
+  uint32_t cand = tag_match(m, rep);
   *val = 0;
-  if constexpr (kHome) {
-    // the meta sector and the home group's keys in one round trip
-    const uint32_t g = home_group<Tr>(h);
-    const HomeKeys<Tr> hk = load_home<Tr>(slab, g);
-    cand = tag_match(m, rep);
-    constexpr uint32_t kHomeMask = (1u << Tr::kHomeSlots) - 1u;
-    const uint32_t hs = g * Tr::kHomeSlots;
-    const int j = home_slot<Tr>(hk, (cand >> hs) & kHomeMask, key);
-    if (j >= 0) {
-      // the value shares the key's sector, which the key load brought to L1
-      if constexpr (Tr::kHasValue)
-        *val = ld_ca_u64(slab + kMetaBytes + (hs + (uint32_t)j) * Tr::kSlotBytes + 8);
-      return true;
-    }
-    cand &= ~(kHomeMask << hs);
-  } else {
-    cand = tag_match(m, rep);
-  }
   bool found = false;
   if (cand) {
     const int slot = __ffs(cand) - 1;
@@ -593,29 +503,21 @@ __device__ __forceinline__ bool read_lookup(const TableView& t, typename Tr::Key
   return found;
 }
 
-// P independent lookups issued together: all head meta sectors and home
-// groups first, then each lookup's value (a home hit, from L1) or first
-// other candidate slot, so a thread keeps up to 3P loads in flight.  The
-// rare rest (another candidate, a longer chain) falls back to find_rest.
-template <class Tr, int P, bool kHome = true>
+// P independent lookups issued together: all head meta sectors first, then
+// all first-candidate slots, so a thread keeps up to P loads in flight.  The
+// rare rest (second candidate, longer chain) falls back to find_rest.
+template <class Tr, int P>
 __device__ __forceinline__ void table_find_n(const TableView& t, const typename Tr::Key* key,
                                              const uint64_t* h, const bool* want, bool* found,
                                              uint64_t* val, uint64_t* loc) {
-  constexpr uint32_t kHomeMask = kHome ? (1u << Tr::kHomeSlots) - 1u : 0u;
   Meta m[P];
-  HomeKeys<Tr> hk[P];
-  uint32_t rep[P], s[P], cand[P], hs[P], next[P];
+  uint32_t rep[P], s[P], cand[P], next[P];
   const uint8_t* base = (const uint8_t*)t.slabs;
 #pragma unroll
   for (int j = 0; j < P; ++j) {
     s[j] = (uint32_t)h[j] & t.mask;
     rep[j] = (0x80u | fingerprint(h[j])) * 0x01010101u;
-    hs[j] = home_group<Tr>(h[j]) * Tr::kHomeSlots;
-    if (want[j]) {
-      const uint8_t* slab = slab_ptr(base, s[j], Tr::kSlabBytes);
-      m[j] = load_meta<true>(slab);
-      if (kHome) hk[j] = load_home<Tr>(slab, hs[j] / Tr::kHomeSlots);
-    }
+    if (want[j]) m[j] = load_meta<true>(slab_ptr(base, s[j], Tr::kSlabBytes));
   }
   uint64_t k0[P], v0[P];
   int slot0[P];
@@ -623,24 +525,15 @@ __device__ __forceinline__ void table_find_n(const TableView& t, const typename 
   for (int j = 0; j < P; ++j) {
     cand[j] = want[j] ? tag_match(m[j], rep[j]) : 0u;
     next[j] = want[j] ? m[j].next : 0u;
-    const int hj =
-        kHome && want[j] ? home_slot<Tr>(hk[j], (cand[j] >> hs[j]) & kHomeMask, key[j]) : -1;
-    const uint8_t* sp = slab_ptr(base, s[j], Tr::kSlabBytes) + kMetaBytes;
-    if (hj >= 0) {  // home hit: the value from the sector the key load brought in
-      slot0[j] = (int)hs[j] + hj;
-      k0[j] = (uint64_t)key[j];
-      v0[j] = Tr::kHasValue ? ld_ca_u64(sp + slot0[j] * Tr::kSlotBytes + 8) : 0ull;
-      continue;
-    }
-    cand[j] &= ~(kHomeMask << hs[j]);
     slot0[j] = cand[j] ? __ffs(cand[j]) - 1 : -1;
     if (slot0[j] >= 0) {
+      const uint8_t* sp = slab_ptr(base, s[j], Tr::kSlabBytes) + kMetaBytes + slot0[j] * Tr::kSlotBytes;
       if constexpr (Tr::kHasValue) {
-        ulonglong2 kv = ld_ca_v2u64(sp + slot0[j] * Tr::kSlotBytes);
+        ulonglong2 kv = ld_ca_v2u64(sp);
         k0[j] = kv.x;
         v0[j] = kv.y;
       } else {
-        k0[j] = ld_ca_u32(sp + slot0[j] * Tr::kSlotBytes);
+        k0[j] = ld_ca_u32(sp);
         v0[j] = 0;
       }
     }
@@ -741,13 +634,8 @@ __device__ __forceinline__ bool scan_chain(const TableView& t, typename Tr::Key 
       }
       fr &= (1u << kSlots) - 1u;
       if (fr) {
-        // in the head slab, a free slot of the key's home group first
-        constexpr uint32_t kHomeMask = (1u << Tr::kHomeSlots) - 1u;
-        const uint32_t home = s == ((uint32_t)h & t.mask)
-                                  ? fr & (kHomeMask << (home_group<Tr>(h) * Tr::kHomeSlots))
-                                  : 0u;
         r.free_slab = s;
-        r.free_slot = __ffs(home ? home : fr) - 1;
+        r.free_slot = __ffs(fr) - 1;
       }
     }
     r.tail = s;

@@ -340,10 +340,8 @@ struct ProbeSel {
 
 // Probe (and, for mutations, group) the ops idx[j] whose type and key the
 // caller loaded; lanes in ascending op-index order.  Every lane of the warp
-// calls it.  kHome: load each key's home group beside its meta sector (one
-// round trip for most hits; the stand-alone probe kernels do, the
-// persistent kernels, whose registers are spent elsewhere, do not).
-template <class Tr, bool kGroup, int P, bool kHome = false>
+// calls it.
+template <class Tr, bool kGroup, int P>
 __device__ __forceinline__ void probe_ops(const TableView& t, const Scratch& sc,
                                           const Window<Tr>& w, uint32_t lane, bool dedup,
                                           const uint32_t (&idx)[P], const uint8_t (&type)[P],
@@ -379,7 +377,7 @@ __device__ __forceinline__ void probe_ops(const TableView& t, const Scratch& sc,
       }
     }
   } else {
-    table_find_n<Tr, P, kHome>(t, key, h, want, found, value, loc);
+    table_find_n<Tr, P>(t, key, h, want, found, value, loc);
   }
 #pragma unroll
   for (int j = 0; j < P; ++j) {
@@ -426,7 +424,7 @@ __device__ __forceinline__ void probe_ops(const TableView& t, const Scratch& sc,
 // Ops base + j*32 + lane, j < P.  `perm` (optional): position -> op index
 // (the binned order); positions are then mapped to ops, and sel's read range
 // is in positions.
-template <class Tr, bool kGroup, int P, bool kHome = false>
+template <class Tr, bool kGroup, int P>
 __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc,
                                            const Window<Tr>& w, uint32_t base, uint32_t lane,
                                            bool dedup, const ProbeSel& sel,
@@ -446,7 +444,7 @@ __device__ __forceinline__ void probe_tile(const TableView& t, const Scratch& sc
     active[j] = i < w.n && (type[j] == kOpRead ? (pos >= sel.read_lo && pos < sel.read_hi) : sel.muts);
     key[j] = active[j] ? (perm ? key_of(w, i) : key_stream(w, i)) : (Key)0;
   }
-  probe_ops<Tr, kGroup, P, kHome>(t, sc, w, lane, dedup, idx, type, active, key);
+  probe_ops<Tr, kGroup, P>(t, sc, w, lane, dedup, idx, type, active, key);
 }
 
 // Phase A for the mutations of a window (its reads are probed by blocks
@@ -512,7 +510,7 @@ __device__ void phase_list_muts(const Scratch& sc, const Window<Tr>& w, uint32_t
   }
 }
 
-template <class Tr, bool kHome = false>
+template <class Tr>
 __device__ void phase_probe_list(const TableView& t, const Scratch& sc, const Window<Tr>& w,
                                  uint32_t warp_id, uint32_t num_warps, bool dedup) {
   using Key = typename Tr::Key;
@@ -530,7 +528,7 @@ __device__ void phase_probe_list(const TableView& t, const Scratch& sc, const Wi
       active[0] = type[0] != kOpRead;
       key[0] = key_of(w, i);
     }
-    probe_ops<Tr, true, 1, kHome>(t, sc, w, lane, dedup, idx, type, active, key);
+    probe_ops<Tr, true, 1>(t, sc, w, lane, dedup, idx, type, active, key);
     if (lane == 0) atomicAdd(&w.cnt->tiles_done, 1u);
   }
 }
@@ -543,7 +541,7 @@ __device__ void phase_probe_list(const TableView& t, const Scratch& sc, const Wi
 // tile).  With `stop_at`, a block takes no further chunk once *stop_at has
 // reached stop_target (the rest is claimed by a later call on the same
 // cursor).  Every thread of the block must call it.
-template <class Tr, bool kGroup, int P, bool kHome = false>
+template <class Tr, bool kGroup, int P>
 __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<Tr>& w,
                             uint32_t warp_id, uint32_t num_warps, uint32_t* cursor,
                             uint32_t chunk, bool dedup,
@@ -553,7 +551,7 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
   const uint32_t lane = lane_id();
   if (cursor == nullptr || chunk == 0) {
     for (uint32_t base = begin + warp_id * 32 * P; base < w.n; base += num_warps * 32 * P)
-      probe_tile<Tr, kGroup, P, kHome>(t, sc, w, base, lane, dedup, sel, perm);
+      probe_tile<Tr, kGroup, P>(t, sc, w, base, lane, dedup, sel, perm);
     return;
   }
   __shared__ uint32_t s_base, s_next;
@@ -577,7 +575,7 @@ __device__ void phase_probe(const TableView& t, const Scratch& sc, const Window<
       if (lane == 0) off = atomicAdd(&s_next, 32u * P);
       off = __shfl_sync(0xFFFFFFFFu, off, 0);
       if (c0 + off >= c1) break;
-      probe_tile<Tr, kGroup, P, kHome>(t, sc, w, c0 + off, lane, dedup, sel, perm);
+      probe_tile<Tr, kGroup, P>(t, sc, w, c0 + off, lane, dedup, sel, perm);
     }
     __syncthreads();  // s_base / s_next are rewritten next round
   }

@@ -30,7 +30,6 @@ inline uint64_t l2_keep() { return 0; }
 inline uint4 ld_ca_v4(const void* p) { return ld_cg_v4(p); }
 inline ulonglong2 ld_ca_v2u64(const void* p) { return ld_cg_v2u64(p); }
 inline uint32_t ld_ca_u32(const void* p) { return ld_cg_u32(p); }
-inline uint64_t ld_ca_u64(const void* p) { return ld_cg_u64(p); }
 inline uint64_t ld_cs_u64(const void* p) { return emu_detail::ld<uint64_t>(p); }
 inline uint32_t ld_cs_u32(const void* p) { return emu_detail::ld<uint32_t>(p); }
 inline uint8_t ld_cs_u8(const void* p) { return emu_detail::ld<uint8_t>(p); }
