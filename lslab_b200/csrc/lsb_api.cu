@@ -62,18 +62,15 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 // (a grid-stride grid that leaves room on every SM for the mutation steps;
 // 0 = one thread per op).  Measured on the 2^20-op 95/5 batch (per batch):
 // 1/0 75.8 us, 1/4 78.6, 1/6 81.8, 1/7 79.6, 0/6 101.9; per-op-type calls
-// 77.8 us.
+// 77.8 us.  With the resolve launch held to one wave of blocks: 1/0
+// 69.6-70.7 us; the reads started after the listing 70.5-71.3; the
+// mutations probed in op order by warps that skip tiles of reads (no list,
+// an epoch-check kernel first) 73.8-74.4; per-op-type calls 77.1-77.3.
 #ifndef LSB_OVERLAP_SPLIT
 #define LSB_OVERLAP_SPLIT 1
 #endif
 #ifndef LSB_OVERLAP_READ_BLOCKS
 #define LSB_OVERLAP_READ_BLOCKS 0
-#endif
-// LSB_OVERLAP_READ_WAIT 1: the read kernel starts once the mutation list is
-// built, so the probe-and-group kernel (higher stream priority) takes its
-// blocks before the reads fill the SMs; 0: the reads start with the window.
-#ifndef LSB_OVERLAP_READ_WAIT
-#define LSB_OVERLAP_READ_WAIT 0
 #endif
 // threads per block of the ordering kernel k_sort (one block per SM; a
 // block orders one big group at a time)
@@ -1067,7 +1064,7 @@ struct Table {
   // tuning overlap: the mutation steps of a window run on `side` (highest
   // stream priority, so its blocks take SMs as k_read's blocks retire)
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_list = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint32_t* rhist = nullptr;  // region counts of ordered reads (+ the read count)
   // Tracing of the two-stream form: per window, timing events at its start
   // and after each of its kernels (kSpanPoints points, kSpanWindows windows
@@ -1099,7 +1096,6 @@ struct Table {
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
-    if (ev_list) cudaEventDestroy(ev_list);
     destroy_spans();
   }
 
@@ -1220,7 +1216,6 @@ struct Table {
     LSB_CK(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, greatest));
     LSB_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     LSB_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
-    LSB_CK(cudaEventCreateWithFlags(&ev_list, cudaEventDisableTiming));
     return LSB_OK;
   }
 
@@ -1407,10 +1402,6 @@ struct Table {
           k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256,
                             0, side>>>(sc, w, fused_epoch);
           if (int e2 = span_mark(wi, 1, side)) return e2;
-          if (LSB_OVERLAP_READ_WAIT) {
-            LSB_CK(cudaEventRecord(ev_list, side));
-            LSB_CK(cudaStreamWaitEvent(s, ev_list, 0));
-          }
           k_probe_list<Tr><<<num_sms * 2, 256, 0, side>>>(view(), sc, w, fused_epoch);
           if (int e2 = span_mark(wi, 2, side)) return e2;
           if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
