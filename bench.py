@@ -655,6 +655,7 @@ def side_workloads(args, world, rank, local) -> dict:
         at70 = [p for p in sv["sweep"] if abs(p["load"] - 0.7) < 1e-9]
         out[key] = {
             "peak_mops": sv["peak_mops"], "wave_ops": sv["wave_ops"],
+            "peak_wave_split": sv["peak_wave_split"],
             "at_70pct": at70[0] if at70 else None,
             "p99_us_by_load": {str(p["load"]): p["p99_us"] for p in sv["sweep"]},
             "loop_state": sv["loop"]["state"], "device_status": sv["device_status"],
@@ -1015,26 +1016,38 @@ def run_serving(args, world, rank, local):
 
     def run(nreq, arrival):
         idx = rng.integers(0, len(n), size=nreq).astype(np.uint32)
+        q0 = srv.query()
         lat, wall, _ = srv.run_load(arrival, idx, off, n, t, k, v)
+        q1 = srv.query()
         ops = int(n[idx].astype(np.uint64).sum())
-        return lat, wall, ops
+        return lat, wall, ops, wave_split(q0, q1)
+
+    def wave_split(q0, q1):
+        # the loop's own step times over the waves of one run (lsb_serve_query)
+        w = max(1, q1["waves"] - q0["waves"])
+        return {"waves": q1["waves"] - q0["waves"],
+                "ops_per_wave": round((q1["ops"] - q0["ops"]) / w, 1),
+                **{f"{key}_us_per_wave": round((q1[f"{key}_ns"] - q0[f"{key}_ns"]) / w / 1e3, 2)
+                   for key in ("gather", "engine", "tail")},
+                "wait_us_total": round((q1["wait_ns"] - q0["wait_ns"]) / 1e3, 1)}
 
     run(512, np.zeros(512, np.uint64))  # warm-up
     peak_req = 8192
-    _, wall, ops = run(peak_req, np.zeros(peak_req, np.uint64))
+    _, wall, ops, peak_split = run(peak_req, np.zeros(peak_req, np.uint64))
     peak = ops / (wall * 1e-9)
     sweep = []
     for f in [float(x) for x in args.serve_loads.split(",")]:
         lam = f * peak / mean_n  # requests per second
         nreq = max(256, int(lam * args.serve_seconds))
         arrival = np.cumsum(rng.exponential(1e9 / lam, size=nreq)).astype(np.uint64)
-        lat, wall, ops = run(nreq, arrival)
+        lat, wall, ops, split = run(nreq, arrival)
         us = lat / 1e3
         sweep.append({"load": f, "offered_mops": round(f * peak / 1e6, 1),
                       "achieved_mops": round(ops / (wall * 1e-9) / 1e6, 1), "requests": nreq,
                       "p50_us": round(float(np.percentile(us, 50)), 1),
                       "p99_us": round(float(np.percentile(us, 99)), 1),
-                      "p999_us": round(float(np.percentile(us, 99.9)), 1)})
+                      "p999_us": round(float(np.percentile(us, 99.9)), 1),
+                      "wave_split": split})
     stats = srv.stop()
     srv.close()
     at70 = [p for p in sweep if abs(p["load"] - 0.7) < 1e-9]
@@ -1043,7 +1056,7 @@ def run_serving(args, world, rank, local):
         "description": ("map 2^25 buckets, slab pool capped at 24 GB; requests uniform [1, 4096] "
                         "ops, 50/50 get/put, Zipf 0.99 over 2^28 keys; open-loop Poisson "
                         "arrivals; latency = scheduled arrival to observed completion"),
-        "wave_ops": args.wave_ops, "peak_mops": round(peak / 1e6, 1),
+        "wave_ops": args.wave_ops, "peak_mops": round(peak / 1e6, 1), "peak_wave_split": peak_split,
         "p99_us_at_70pct": at70[0]["p99_us"] if at70 else None,
         "sweep": sweep, "loop": stats, "device_status": m.status(),
         "pool_slabs_used": m.pool_usage()[0],

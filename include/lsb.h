@@ -400,6 +400,15 @@ typedef struct lsb_serve_stats {
   uint32_t state;     /* 0 never ran, 1 running, 2 drained after stop, 3 idle limit,
                          4 a grid barrier gave up (see lsb_map_status) */
   uint32_t pad;
+  /* Device time of the loop by step, ns summed over all waves (one device
+   * thread's %globaltimer): gathering a wave's ops from the host-mapped
+   * arena; the engine (probe, ordering, resolve); the tail (the rest of the
+   * resolve, admitting the next wave, the last barrier); waiting for
+   * requests while the queue was empty. */
+  uint64_t gather_ns;
+  uint64_t engine_ns;
+  uint64_t tail_ns;
+  uint64_t wait_ns;
 } lsb_serve_stats;
 
 int lsb_serve_create(lsb_map* m, const lsb_serve_options* opt, lsb_server** out);
@@ -418,6 +427,11 @@ int lsb_serve_poll(lsb_server* s, uint64_t ticket, int* done);
 int lsb_serve_take(lsb_server* s, uint64_t ticket, lsb_result* out, int* status);
 /* Drains the queue, ends the loop, waits for it.  Synchronises. */
 int lsb_serve_stop(lsb_server* s, lsb_serve_stats* stats);
+/* The loop's counters so far, read while it runs (no synchronisation; each
+ * field is as of the last completed wave).  Differences of two snapshots
+ * give the counts and step times of the waves in between.  No reference
+ * counterpart (serving has none). */
+int lsb_serve_query(lsb_server* s, lsb_serve_stats* stats);
 int lsb_serve_destroy(lsb_server* s);
 
 /* Open-loop load generator for the serving benchmark: issues nreq requests

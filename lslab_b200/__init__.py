@@ -399,10 +399,22 @@ class Server:
                    "lsb_serve_run_load")
         return lat, int(wall.value), res
 
+    @staticmethod
+    def _stats(s) -> dict:
+        return {"waves": s.waves, "ops": s.ops, "requests": s.requests, "state": s.state,
+                "gather_ns": s.gather_ns, "engine_ns": s.engine_ns, "tail_ns": s.tail_ns,
+                "wait_ns": s.wait_ns}
+
     def stop(self) -> dict:
         s = _lib.ServeStats()
         _lib.check(lib().lsb_serve_stop(self._h, C.byref(s)), "lsb_serve_stop")
-        return {"waves": s.waves, "ops": s.ops, "requests": s.requests, "state": s.state}
+        return self._stats(s)
+
+    def query(self) -> dict:
+        """The running loop's counters and step times so far (lsb_serve_query)."""
+        s = _lib.ServeStats()
+        _lib.check(lib().lsb_serve_query(self._h, C.byref(s)), "lsb_serve_query")
+        return self._stats(s)
 
     def close(self):
         if self._h is not None:

@@ -99,6 +99,10 @@ class ServeStats(C.Structure):
         ("requests", C.c_uint64),
         ("state", C.c_uint32),
         ("pad", C.c_uint32),
+        ("gather_ns", C.c_uint64),
+        ("engine_ns", C.c_uint64),
+        ("tail_ns", C.c_uint64),
+        ("wait_ns", C.c_uint64),
     ]
 
 
@@ -198,6 +202,7 @@ _SIGS = {
     "lsb_serve_poll": (C.c_int, [_P, _U64, C.POINTER(C.c_int)]),
     "lsb_serve_take": (C.c_int, [_P, _U64, _P, C.POINTER(C.c_int)]),
     "lsb_serve_stop": (C.c_int, [_P, C.POINTER(ServeStats)]),
+    "lsb_serve_query": (C.c_int, [_P, C.POINTER(ServeStats)]),
     "lsb_serve_destroy": (C.c_int, [_P]),
     "lsb_serve_run_load": (C.c_int, [_P, C.POINTER(ServeLoad), _P, C.POINTER(_U64)]),
     "lsb_error_string": (C.c_char_p, [C.c_int]),

@@ -638,6 +638,12 @@ struct ServeCtl {     // host-mapped
   uint64_t ops;        // ops run
   uint32_t stop;       // host: end the loop once the queue is drained
   uint32_t state;      // device: see lsb_serve_stats.state
+  // device: %globaltimer ns summed over waves by one timing thread (block 0,
+  // thread 32, which takes part in every step but the admission), rewritten
+  // after every wave: gather, engine (probe, ordering, its resolve share),
+  // tail (the rest of the resolve, the admission, the last barrier), and the
+  // waits for requests when the queue ran empty
+  uint64_t t_gather, t_engine, t_tail, t_wait;
 };
 
 struct ServeReq {     // one request slot, host-mapped
@@ -862,6 +868,43 @@ struct AdmitNext {
   __device__ void operator()() const { serve_admit(*t, *j, out, head, false, in_flight_puts); }
 };
 
+// A wave's ops from the host-mapped arena into HBM, thread t of nt.  Loads
+// are volatile (.cv: the host rewrites arena slots between waves) and 16
+// bytes wide where the source is 16-byte aligned, so a warp's loads cross
+// PCIe as 512-byte requests; the ragged ends take scalar loads, so nothing
+// outside [src, src + n) is read.  (One 1-, 8- and 8-byte load per op per
+// thread moved 10-14 GB/s: 40 us of a 25k-op wave.)
+__device__ __forceinline__ void gather_u64(const uint64_t* src, uint64_t* dst, uint32_t n,
+                                           uint32_t t, uint32_t nt) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  const uint32_t h = (((uintptr_t)src & 15u) != 0 && n != 0) ? 1u : 0u;  // to 16-B alignment
+  const uint32_t pairs = (n - h) / 2;
+  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(s + h);
+  for (uint32_t p = t; p < pairs; p += nt) {
+    const ulonglong2 v = __ldcv(s2 + p);
+    dst[h + 2 * p] = v.x;
+    dst[h + 2 * p + 1] = v.y;
+  }
+  if (h && t == 0) dst[0] = __ldcv(s);
+  if (((n - h) & 1u) && t == nt - 1) dst[n - 1] = __ldcv(s + n - 1);
+}
+
+__device__ __forceinline__ void gather_u8(const uint8_t* src, uint8_t* dst, uint32_t n, uint32_t t,
+                                          uint32_t nt) {
+  const uint32_t h = min(n, (uint32_t)((16u - ((uintptr_t)src & 15u)) & 15u));
+  const uint32_t chunks = (n - h) / 16;
+  const uint4* s4 = reinterpret_cast<const uint4*>(src + h);
+  for (uint32_t c = t; c < chunks; c += nt) {
+    const uint4 v = __ldcv(s4 + c);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    uint8_t* d = dst + h + 16 * c;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) d[q] = (uint8_t)(w[q >> 2] >> (8 * (q & 3)));
+  }
+  for (uint32_t i = t; i < h; i += nt) dst[i] = __ldcv(src + i);
+  for (uint32_t i = h + 16 * chunks + t; i < n; i += nt) dst[i] = __ldcv(src + i);
+}
+
 template <int P>
 __global__ void __launch_bounds__(1024, 1)
     k_serve(TableView t, Scratch sc, ServeJob j, GridBarrier* bar) {
@@ -877,6 +920,14 @@ __global__ void __launch_bounds__(1024, 1)
     ops = *(volatile uint64_t*)&j.ctl->ops;
   }
   if (tid == 0) *(volatile uint32_t*)&j.ctl->state = 1;
+  const bool timer = blockIdx.x == 0 && threadIdx.x == 32;
+  uint64_t tg = 0, te = 0, tt = 0, tw = 0;  // the timing thread's sums
+  if (timer) {
+    tg = *(volatile uint64_t*)&j.ctl->t_gather;
+    te = *(volatile uint64_t*)&j.ctl->t_engine;
+    tt = *(volatile uint64_t*)&j.ctl->t_tail;
+    tw = *(volatile uint64_t*)&j.ctl->t_wait;
+  }
   // Wave k+1 is admitted (without waiting) as wave k's last phase ends, so
   // one grid barrier both completes wave k and publishes wave k+1; only an
   // empty queue makes warp 0 wait for requests, after wave k is published.
@@ -890,6 +941,8 @@ __global__ void __launch_bounds__(1024, 1)
   if (!grid_barrier_until(bar, gridDim.x, t.status, seq, global_ns() + j.idle_ns + kAdmitMarginNs))
     goto out;
   for (;;) {
+    const uint64_t t0 = timer ? global_ns() : 0;
+    uint64_t t1 = t0, t2 = t0;
     const WaveDesc* cur = &j.wave[a & 1];
     const uint64_t first = ld_cg_u64(&cur->first), op_off = ld_cg_u64(&cur->op_off);
     const uint32_t nreq = ld_cg_u32(&cur->nreq), nops = ld_cg_u32(&cur->nops);
@@ -907,16 +960,11 @@ __global__ void __launch_bounds__(1024, 1)
       // the wave's ops (contiguous in one lap of the arena) into HBM; .cv
       // loads because the host rewrites arena slots between waves
       const uint64_t pos = op_off % j.arena_cap;
-      for (uint32_t i = tid; i < nops; i += nt) {
-        // all three loads before any store: they cross PCIe together
-        const uint8_t ty = __ldcv(j.a_types + pos + i);
-        const uint64_t key = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_keys) + pos + i);
-        const uint64_t val = __ldcv(reinterpret_cast<const unsigned long long*>(j.a_vals) + pos + i);
-        j.d_types[i] = ty;
-        j.d_keys[i] = key;
-        j.d_vals[i] = val;
-      }
+      gather_u64(j.a_keys + pos, j.d_keys, nops, tid, nt);
+      gather_u64(j.a_vals + pos, j.d_vals, nops, tid, nt);
+      gather_u8(j.a_types + pos, j.d_types, nops, tid, nt);
       if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+      if (timer) t1 = global_ns();
       FusedJob<MapTraits> fj = j.fj;
       fj.base.types = j.d_types;
       fj.base.keys = j.d_keys;
@@ -927,11 +975,20 @@ __global__ void __launch_bounds__(1024, 1)
       fused_windows<MapTraits, P, false>(
           t, sc, fj, bar, smem, seq,
           AdmitNext{&t, &j, &j.wave[(a + 1) & 1], first + nreq, wave_puts});
+      if (timer) t2 = global_ns();
     }
     const uint64_t next = first + nreq;
     ++a;
     if (tid < 32 && nops == 0) serve_admit(t, j, &j.wave[a & 1], next, false, wave_puts);
     if (!grid_barrier(bar, gridDim.x, t.status, seq)) break;
+    if (timer) {
+      tg += t1 - t0;
+      te += t2 - t1;
+      tt += global_ns() - t2;
+      *(volatile uint64_t*)&j.ctl->t_gather = tg;
+      *(volatile uint64_t*)&j.ctl->t_engine = te;
+      *(volatile uint64_t*)&j.ctl->t_tail = tt;
+    }
     if (tid == 0) {
       win_counters_reset(&sc.cnt[0]);  // the next wave's counters (visible after its barrier)
       __threadfence_system();          // results before the completion count
@@ -944,10 +1001,15 @@ __global__ void __launch_bounds__(1024, 1)
     if (ld_cg_u32(&j.wave[a & 1].nreq) == 0 && ld_cg_u32(&j.wave[a & 1].stop) == 0) {
       // the queue was empty: wait for requests now that wave k is published
       ++a;
+      const uint64_t t3 = timer ? global_ns() : 0;
       if (tid < 32) serve_admit(t, j, &j.wave[a & 1], next, true, 0);
       if (!grid_barrier_until(bar, gridDim.x, t.status, seq,
                               global_ns() + j.idle_ns + kAdmitMarginNs))
         break;
+      if (timer) {
+        tw += global_ns() - t3;
+        *(volatile uint64_t*)&j.ctl->t_wait = tw;
+      }
     }
   }
 out:
@@ -2477,14 +2539,23 @@ int lsb_serve_stop(lsb_server* s, lsb_serve_stats* stats) {
     if (cudaStreamSynchronize(s->stream) != cudaSuccess) rc = LSB_ERR_CUDA;
     s->running = false;
   }
-  if (stats) {
-    stats->waves = s->ctl->waves;
-    stats->ops = s->ctl->ops;
-    stats->requests = s->ctl->completed;
-    stats->state = s->ctl->state;
-    stats->pad = 0;
-  }
+  if (stats) lsb_serve_query(s, stats);
   return rc;
+}
+
+int lsb_serve_query(lsb_server* s, lsb_serve_stats* stats) {
+  if (!s || !stats) return LSB_ERR_ARG;
+  volatile ServeCtl* c = s->ctl;
+  stats->waves = c->waves;
+  stats->ops = c->ops;
+  stats->requests = c->completed;
+  stats->state = c->state;
+  stats->pad = 0;
+  stats->gather_ns = c->t_gather;
+  stats->engine_ns = c->t_engine;
+  stats->tail_ns = c->t_tail;
+  stats->wait_ns = c->t_wait;
+  return LSB_OK;
 }
 
 int lsb_serve_destroy(lsb_server* s) {

@@ -154,11 +154,22 @@ def test_serve_open_loop_generator(cuda):
     m = Map(8, max_window=1 << 16)
     srv = Server(m, max_wave_ops=1 << 14, ring_requests=256, arena_ops=1 << 16)
     srv.start()
+    q0 = srv.query()
     lat, wall, res = srv.run_load(arrival, idx, pool_off, pool_n, t, k, v, want_results=True)
+    q1 = srv.query()
     stats = srv.stop()
     srv.close()
     assert stats["requests"] == nreq
     assert (lat > 0).all() and wall > 0
+    # the loop's step times (lsb_serve_query): every wave has gather, engine
+    # and tail time, the sums only grow, and stop reports at least as much
+    assert q1["waves"] > q0["waves"] and q1["requests"] == nreq
+    for key in ("gather_ns", "engine_ns", "tail_ns"):
+        assert q1[key] > q0[key], key
+        assert stats[key] >= q1[key], key
+    # the three steps of the waves fit inside the run's wall time
+    busy = sum(q1[key] - q0[key] for key in ("gather_ns", "engine_ns", "tail_ns"))
+    assert busy <= wall * 1.05 + 1_000_000
     seq = [slice(int(pool_off[i]), int(pool_off[i]) + int(pool_n[i])) for i in idx]
     want = OracleMap(8).mixed(np.concatenate([t[s] for s in seq]), np.concatenate([k[s] for s in seq]),
                               np.concatenate([v[s] for s in seq]))
