@@ -960,6 +960,9 @@ __global__ void __launch_bounds__(1024, 1)
       // the wave's ops (contiguous in one lap of the arena) into HBM; .cv
       // loads because the host rewrites arena slots between waves
       const uint64_t pos = op_off % j.arena_cap;
+      // (Gathering the values during the probe instead, by the threads that
+      // probe no op, measured no faster per op: the probe's barrier waited
+      // for their PCIe loads.)
       gather_u64(j.a_keys + pos, j.d_keys, nops, tid, nt);
       gather_u64(j.a_vals + pos, j.d_vals, nops, tid, nt);
       gather_u8(j.a_types + pos, j.d_types, nops, tid, nt);

@@ -155,3 +155,32 @@ def test_overlap_graph_replays_through_epoch_wrap(cuda):
             assert same_results(got2, want2), f"fused after {r}: " + first_mismatch(got2, want2)
     g.close()
     _check_map(m, o, results(out), want)
+
+
+def test_overlap_trace_spans(cuda):
+    """With tracing on, a two-stream call records each window's start, its
+    read kernel, listing, probing, ordering and resolve ends (timing events,
+    lsb_map_read_trace); the steps on each stream end in order, the resolve
+    last, and the results stay exact."""
+    n, log2 = 20_000, 8
+    types, keys, vals = _mixed(11, n, key_space=500)
+    o = OracleMap(log2)
+    want = o.mixed(types, keys, vals)
+    m = Map(log2, max_window=8192)
+    m.set_tuning(overlap=1)
+    m.set_trace(True)
+    out = results_buf(n)
+    m.execute_fused(dev(types), dev(keys), dev(vals), out)
+    tr = m.read_trace()
+    _sync()
+    assert same_results(results(out), want), first_mismatch(results(out), want)
+    nwin = -(-n // 8192)
+    assert len(tr) == 6 * nwin
+    for wi in range(nwin):
+        pts = {(w, ph): ns for ns, w, ph in tr if (w & 31) == wi}
+        start, reads, muts, done = pts[(wi, 0)], pts[(wi, 1)], pts[(wi, 2)], pts[(wi, 3)]
+        listed, probed = pts[(wi | 32, 1)], pts[(wi | 32, 2)]
+        assert start <= listed <= probed <= muts <= done
+        assert start <= reads <= done
+    m.set_trace(False)
+    assert m.status() == 0
