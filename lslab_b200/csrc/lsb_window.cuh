@@ -1406,10 +1406,16 @@ __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
   for (uint32_t j = tid; j < mcount; j += nthreads) {
     const uint32_t m = ld_cg_u32(&sc.mlist[j]);
     if (m >= w.n) continue;
+    // everything that depends on m alone in one round trip: the group slot,
+    // the op, the slot location its probe found and its ordering record
+    // (only meaningful, and only used, in groups of more than kInline)
     const uint64_t mi = ld_cg_u64(&sc.minfo[m]);
+    const uint64_t loc = ld_cg_u64(&sc.mloc[m]);
+    const uint32_t prec = ld_cg_u32(&sc.pred[m]);
+    const uint8_t type = op_type(w, m);
+    const typename Tr::Key key = key_of(w, m);
     const uint32_t gslot = (uint32_t)(mi >> 32) & sc.gmask;
     const uint32_t c = g_count(ld_relaxed_u64(&sc.gtab[gslot]));
-    const uint8_t type = op_type(w, m);
     uint32_t pred;
     bool last = true;
     if (c == 1) {
@@ -1417,9 +1423,8 @@ __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
     } else if (c <= kInline) {
       pred = inline_pred(sc, gslot, c, m, w.n, &last);
     } else {
-      const uint32_t p = ld_cg_u32(&sc.pred[m]);
-      pred = (p & kPredMask) ? (p & kPredMask) - 1 : 0xFFFFFFFFu;
-      last = (p & kPredLast) != 0;
+      pred = (prec & kPredMask) ? (prec & kPredMask) - 1 : 0xFFFFFFFFu;
+      last = (prec & kPredLast) != 0;
     }
     if (pred < w.n) {
       bool present;
@@ -1428,11 +1433,10 @@ __device__ void phase_resolve_mutations(const TableView& t, const Scratch& sc,
       write_result(w, m, type, present, value);
     }
     if (last) {
-      const typename Tr::Key key = key_of(w, m);
       bool present = type == kOpWrite;
       if (type == kOpUpdate) present = present_before<Tr>(sc, w, gslot, c, m);
       const uint64_t val = (Tr::kHasValue && present) ? val_of(w, m) : 0ull;
-      table_apply_known<Tr>(t, key, Tr::hash(key), ld_cg_u64(&sc.mloc[m]), present, val);
+      table_apply_known<Tr>(t, key, Tr::hash(key), loc, present, val);
     }
   }
 }
