@@ -13,6 +13,7 @@
 
 #include "lsb.h"
 #include "lsb_core.cuh"
+#include "lsb_gather.cuh"
 #include "lsb_internal.h"
 #include "lsb_window.cuh"
 
@@ -843,43 +844,6 @@ struct AdmitNext {
   uint64_t in_flight_puts;
   __device__ void operator()() const { serve_admit(*t, *j, out, head, false, in_flight_puts); }
 };
-
-// A wave's ops from the host-mapped arena into HBM, thread t of nt.  Loads
-// are volatile (.cv: the host rewrites arena slots between waves) and 16
-// bytes wide where the source is 16-byte aligned, so a warp's loads cross
-// PCIe as 512-byte requests; the ragged ends take scalar loads, so nothing
-// outside [src, src + n) is read.  (One 1-, 8- and 8-byte load per op per
-// thread moved 10-14 GB/s: 40 us of a 25k-op wave.)
-__device__ __forceinline__ void gather_u64(const uint64_t* src, uint64_t* dst, uint32_t n,
-                                           uint32_t t, uint32_t nt) {
-  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
-  const uint32_t h = (((uintptr_t)src & 15u) != 0 && n != 0) ? 1u : 0u;  // to 16-B alignment
-  const uint32_t pairs = (n - h) / 2;
-  const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(s + h);
-  for (uint32_t p = t; p < pairs; p += nt) {
-    const ulonglong2 v = __ldcv(s2 + p);
-    dst[h + 2 * p] = v.x;
-    dst[h + 2 * p + 1] = v.y;
-  }
-  if (h && t == 0) dst[0] = __ldcv(s);
-  if (((n - h) & 1u) && t == nt - 1) dst[n - 1] = __ldcv(s + n - 1);
-}
-
-__device__ __forceinline__ void gather_u8(const uint8_t* src, uint8_t* dst, uint32_t n, uint32_t t,
-                                          uint32_t nt) {
-  const uint32_t h = min(n, (uint32_t)((16u - ((uintptr_t)src & 15u)) & 15u));
-  const uint32_t chunks = (n - h) / 16;
-  const uint4* s4 = reinterpret_cast<const uint4*>(src + h);
-  for (uint32_t c = t; c < chunks; c += nt) {
-    const uint4 v = __ldcv(s4 + c);
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-    uint8_t* d = dst + h + 16 * c;
-#pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = (uint8_t)(w[q >> 2] >> (8 * (q & 3)));
-  }
-  for (uint32_t i = t; i < h; i += nt) dst[i] = __ldcv(src + i);
-  for (uint32_t i = h + 16 * chunks + t; i < n; i += nt) dst[i] = __ldcv(src + i);
-}
 
 template <int P>
 __global__ void __launch_bounds__(1024, 1)

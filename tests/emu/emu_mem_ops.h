@@ -30,6 +30,25 @@ inline uint64_t l2_keep() { return 0; }
 inline uint4 ld_ca_v4(const void* p) { return ld_cg_v4(p); }
 inline ulonglong2 ld_ca_v2u64(const void* p) { return ld_cg_v2u64(p); }
 inline uint32_t ld_ca_u32(const void* p) { return ld_cg_u32(p); }
+// Volatile loads of the serving gather (lsb_gather.cuh).  A test may set
+// emu_read_hook to see every address and width they read.
+inline void (*emu_read_hook)(const void* p, size_t bytes) = nullptr;
+inline uint8_t ld_cv_u8(const uint8_t* p) {
+  if (emu_read_hook) emu_read_hook(p, 1);
+  return emu_detail::ld<uint8_t>(p);
+}
+inline uint64_t ld_cv_u64(const uint64_t* p) {
+  if (emu_read_hook) emu_read_hook(p, 8);
+  return emu_detail::ld<uint64_t>(p);
+}
+inline uint4 ld_cv_v4(const uint4* p) {
+  if (emu_read_hook) emu_read_hook(p, 16);
+  return ld_cg_v4(p);
+}
+inline ulonglong2 ld_cv_v2u64(const ulonglong2* p) {
+  if (emu_read_hook) emu_read_hook(p, 16);
+  return ld_cg_v2u64(p);
+}
 inline uint64_t ld_cs_u64(const void* p) { return emu_detail::ld<uint64_t>(p); }
 inline uint32_t ld_cs_u32(const void* p) { return emu_detail::ld<uint32_t>(p); }
 inline uint8_t ld_cs_u8(const void* p) { return emu_detail::ld<uint8_t>(p); }

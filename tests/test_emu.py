@@ -6,7 +6,8 @@ The window-ordering phase (group formation, per-group ordering including the
 multi-step path for groups of more than 4096 members) is checked against the
 index order it must produce; the whole per-phase batch (probe, ordering,
 resolve) is built with AddressSanitizer, so every access of those phases is
-checked against its buffer, and its results are compared with the oracle."""
+checked against its buffer, and its results are compared with the oracle.
+The serving loop's gather is checked on every source alignment."""
 from __future__ import annotations
 
 import shutil
@@ -272,3 +273,14 @@ def test_v32_put_batch_equals_oracle(bins, tmp_path):
     assert status == 0
     bad = np.nonzero(got != want.astype(np.uint32))[0]
     assert bad.size == 0, f"{bad.size} mismatches, first at {bad[:5]}: {got[bad[:3]]} vs {want[bad[:3]]}"
+
+
+def test_serving_gather_covers_every_alignment(tmp_path):
+    """The serving loop's gather (lsb_gather.cuh, host build under
+    AddressSanitizer): for source offsets 0..31 bytes, 0..200 ops and 1..151
+    threads, the threads together copy the ops exactly once, write nothing
+    past them, read nothing outside them, and load 16 bytes only at aligned
+    addresses."""
+    exe = _build(tmp_path / "gather_emu", "gather_emu.cpp", True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr[-2000:]
