@@ -57,17 +57,19 @@ inline bool aligned(const void* p, size_t a) { return ((uintptr_t)p & (a - 1)) =
 #ifndef LSB_FUSED_LEAN_READS
 #define LSB_FUSED_LEAN_READS 1
 #endif
-// Two-stream window form (tuning overlap): the mutation steps run as three
-// kernels (list, probe from the list, ordering) on a second stream;
-// LSB_OVERLAP_READ_BLOCKS = read-kernel blocks per SM (a grid-stride grid
-// that leaves room on every SM for the mutation steps; 0 = one thread per
-// op).  Measured on the 2^20-op 95/5 batch (per batch): read blocks 0
-// 75.8 us, 4 78.6, 6 81.8, 7 79.6; the mutation steps as one cooperative
-// kernel with grid barriers 101.9; per-op-type calls 77.8 us.  With the
-// resolve launch held to one wave of blocks: 69.6-70.7 us; the reads
-// started after the listing 70.5-71.3; the mutations probed in op order by
-// warps that skip tiles of reads (no list, an epoch-check kernel first)
-// 73.8-74.4; per-op-type calls 77.1-77.3.
+// Two-stream window form (tuning overlap): LSB_OVERLAP_SPLIT 1 = the mutation
+// steps as three kernels (list, probe from the list, ordering), 0 = one
+// cooperative kernel; LSB_OVERLAP_READ_BLOCKS = read-kernel blocks per SM
+// (a grid-stride grid that leaves room on every SM for the mutation steps;
+// 0 = one thread per op).  Measured on the 2^20-op 95/5 batch (per batch):
+// 1/0 75.8 us, 1/4 78.6, 1/6 81.8, 1/7 79.6, 0/6 101.9; per-op-type calls
+// 77.8 us.  With the resolve launch held to one wave of blocks: 1/0
+// 69.6-70.7 us; the reads started after the listing 70.5-71.3; the
+// mutations probed in op order by warps that skip tiles of reads (no list,
+// an epoch-check kernel first) 73.8-74.4; per-op-type calls 77.1-77.3.
+#ifndef LSB_OVERLAP_SPLIT
+#define LSB_OVERLAP_SPLIT 1
+#endif
 #ifndef LSB_OVERLAP_READ_BLOCKS
 #define LSB_OVERLAP_READ_BLOCKS 0
 #endif
@@ -331,28 +333,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Ordering of the window's big groups, and the first hot-key step.  Groups
-// of more than kHugeMin members (hot keys) are counted per index range here
-// (huge_hist); their remaining steps, which need grid barriers, run at the
-// start of k_resolve, a cooperative launch made when the GPU is free (after
-// the join of the two-stream form).  This kernel has no grid barrier, so it
-// is a plain launch whose blocks start as soon as they find room beside the
-// read kernel (a cooperative launch waited for room for all of them at
-// once: 1.5 us a two-stream window).
+// Ordering of the window's big groups; when hot keys produced groups of
+// more than kSortSmall members, the grid (a cooperative launch) continues
+// with the huge_* steps between grid barriers.
 // fused_epoch: the window's epoch is the device one (the two-stream form).
 template <class Tr>
 __global__ void __launch_bounds__(1024, 1)
-    k_sort(Scratch sc, Window<Tr> w, const uint32_t* fused_epoch) {
+    k_sort(Scratch sc, Window<Tr> w, GridBarrier* bar, const uint32_t* fused_epoch) {
   extern __shared__ uint32_t smem[];
   if (fused_epoch != nullptr) w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
   phase_sort_big<Tr>(sc, w, smem);
   if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe kernel has ended
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  uint32_t seq = 0;
   huge_hist<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_scan<Tr>(sc, w, smem);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, sc.status, seq)) return;
+  huge_runs<Tr>(sc, w, smem, gtid, gthreads);
 }
 
 // The mutation steps of the two-stream form as separate kernels of 256-thread
-// blocks: list, then probe and group from the list; the ordering is k_sort.  The window's epoch is the device one.
+// blocks (LSB_OVERLAP_SPLIT 1): list, then probe and group from the list;
+// the ordering is k_sort.  The window's epoch is the device one.
 template <class Tr>
 __global__ void __launch_bounds__(256) k_list_muts(Scratch sc, Window<Tr> w,
                                                    const uint32_t* fused_epoch) {
@@ -372,35 +377,54 @@ __global__ void __launch_bounds__(256, 4)
   phase_probe_list<Tr>(t, sc, w, spread_warp(), (gridDim.x * blockDim.x) >> 5, false);
 }
 
-// Last kernel of a per-phase window, a cooperative launch of at most one
-// wave of blocks.  When hot keys produced groups of more than kHugeMin
-// members, it first finishes their ordering (k_sort counted them per index
-// range): scan, scatter and run sort with grid barriers between them.  Then
-// it resolves, and it leaves the counter block zeroed for the next launch.
-// With fused_epoch (a window on the device epoch), its last block also
-// advances the epoch counter.
+// The mutation steps of a window whose reads run beside it in k_read (the
+// two-stream form, tuning overlap), in one cooperative launch of one
+// 256-thread block per SM, launched first so its blocks are resident before
+// the read kernel takes the rest of each SM: clear the group and chunk
+// tables if the device epochs ran out, list the mutations in op-index order,
+// probe and group them from the list, order the big groups (hot keys by the
+// multi-step grid algorithm), with grid barriers between the steps.  Reads
+// are neither probed nor resolved here.
+template <class Tr>
+__global__ void __launch_bounds__(256, 4)
+    k_mutations(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar,
+                const uint32_t* fused_epoch) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t f = ld_cg_u32(fused_epoch);
+  w.epoch = 2 * dev_window_slot(fused_epoch) + 1;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const uint32_t warp = spread_warp(), nwarps = gthreads >> 5;
+  uint32_t seq = 0;
+  if (f + 1 > kFusedEpochs) {  // grid-uniform: every block read the same counter
+    for (size_t i = gtid; i <= sc.gmask; i += gthreads) sc.gtab[i] = 0;
+    for (size_t i = gtid; i <= sc.cmask; i += gthreads) sc.ctab[i] = 0;
+  }
+  phase_list_muts<Tr>(sc, w, warp, nwarps);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  phase_probe_list<Tr>(t, sc, w, warp, nwarps, false);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  phase_sort_big<Tr>(sc, w, smem);
+  if (huge_groups(sc, w.cnt) == 0) return;  // grid-uniform: the probe step has ended
+  huge_hist<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  huge_scan<Tr>(sc, w, smem);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  huge_scatter<Tr>(sc, w, gtid >> 5, gthreads >> 5);
+  if (!grid_barrier(bar, gridDim.x, t.status, seq)) return;
+  huge_runs<Tr>(sc, w, smem, gtid, gthreads);
+}
+
+// Last kernel of a per-phase window: it also leaves the counter block zeroed
+// for the next launch.  With fused_epoch (a window on the device epoch), its
+// last block also advances the epoch counter.
 template <class Tr>
 __global__ void __launch_bounds__(1024, 1)
     k_resolve(TableView t, Scratch sc, Window<Tr> w, GridBarrier* bar, uint32_t* fused_epoch) {
-  extern __shared__ uint32_t smem[];
   const uint32_t tid = spread_tid(), nt = gridDim.x * blockDim.x;
   const uint32_t slot = fused_epoch != nullptr ? dev_window_slot(fused_epoch) : 0u;
   if (fused_epoch != nullptr) w.epoch = 2 * slot + 1;
-  bool ok = true;
-  if (huge_groups(sc, w.cnt) != 0) {  // grid-uniform: the ordering kernel has ended
-    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t seq = 0;
-    huge_scan<Tr>(sc, w, smem);
-    ok = grid_barrier(bar, gridDim.x, t.status, seq);
-    if (ok) huge_scatter<Tr>(sc, w, gtid >> 5, nt >> 5);
-    ok = ok && grid_barrier(bar, gridDim.x, t.status, seq);
-    if (ok) huge_runs<Tr>(sc, w, smem, gtid, nt);
-    ok = ok && grid_barrier(bar, gridDim.x, t.status, seq);
-  }
-  if (ok) {  // block-uniform (a failed barrier raised the status bit)
-    phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
-    phase_resolve_reads<Tr>(sc, w, tid, nt);
-  }
+  phase_resolve_mutations<Tr>(t, sc, w, tid, nt);
+  phase_resolve_reads<Tr>(sc, w, tid, nt);
   release_counters(sc.cnt, bar, nullptr, 0, fused_epoch, slot + 1);
 }
 
@@ -1206,9 +1230,9 @@ struct Table {
     LSB_CK(cudaMemset(fused_epoch, 0, sizeof(uint32_t)));
     bar = reinterpret_cast<GridBarrier*>(sc.cnt + 2);
     bins = reinterpret_cast<BinCounters*>(reinterpret_cast<uint8_t*>(sc.cnt) + kBinsOffset);
-    LSB_CK(cudaFuncSetAttribute(k_resolve<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_sort<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSortSmemBytes));
+    LSB_CK(cudaFuncSetAttribute(k_mutations<Tr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
     LSB_CK(cudaFuncSetAttribute(k_fused<Tr, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kSortSmemBytes));
@@ -1397,18 +1421,36 @@ struct Table {
         // only reads after a same-key mutation are rewritten by the resolve
         // step, which is also the only step that writes the table.  So the
         // window's reads go through k_read on `s` while the mutation steps
-        // (list, probe and group, order) run on `side` (launched first, at
-        // the highest stream priority: their blocks take SM room as read
-        // blocks retire); the resolve step waits for both.
+        // run in k_mutations on `side` (launched first: its one block per SM
+        // is resident before k_read fills the SMs); the resolve step waits
+        // for both.
         LSB_CK(cudaEventRecord(ev_fork, s));
         LSB_CK(cudaStreamWaitEvent(side, ev_fork, 0));
-        const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
-        k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256,
-                          0, side>>>(sc, w, fused_epoch);
-        if (int e2 = span_mark(wi, 1, side)) return e2;
-        k_probe_list<Tr><<<num_sms * 2, 256, 0, side>>>(view(), sc, w, fused_epoch);
-        if (int e2 = span_mark(wi, 2, side)) return e2;
-        if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
+        if (LSB_OVERLAP_SPLIT) {
+          const uint32_t spans = (m + kListSpan - 1) / kListSpan;  // a warp per 512-op span
+          k_list_muts<Tr><<<std::max(1u, std::min<uint32_t>((spans + 7) / 8, num_sms * 8)), 256,
+                            0, side>>>(sc, w, fused_epoch);
+          if (int e2 = span_mark(wi, 1, side)) return e2;
+          k_probe_list<Tr><<<num_sms * 2, 256, 0, side>>>(view(), sc, w, fused_epoch);
+          if (int e2 = span_mark(wi, 2, side)) return e2;
+          if (int e2 = launch_sort(w, side, fused_epoch)) return e2;
+        } else {
+          TableView tv = view();
+          GridBarrier* b = bar;
+          uint32_t* fe = fused_epoch;
+          void* args[] = {&tv, &sc, &w, &b, &fe};
+          cudaLaunchConfig_t cfg = {};
+          cfg.gridDim = dim3(num_sms);
+          cfg.blockDim = dim3(256);
+          cfg.dynamicSmemBytes = kSortSmemBytes;
+          cfg.stream = side;
+          cudaLaunchAttribute attr[1];
+          attr[0].id = cudaLaunchAttributeCooperative;
+          attr[0].val.cooperative = 1;
+          cfg.attrs = attr;
+          cfg.numAttrs = 1;
+          LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_mutations<Tr>, args));
+        }
         if (int e2 = span_mark(wi, 3, side)) return e2;
         LSB_CK(cudaEventRecord(ev_join, side));
         if (ordered_reads(m)) {
@@ -1433,27 +1475,12 @@ struct Table {
       // after the first (20 against 10 us for the 52k puts of a 2^20-op
       // 95/5 window with a grid of one thread per op).
       if (resolve_per_sm == 0 &&
-          (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, k_resolve<Tr>, 256,
-                                                         kSortSmemBytes) != cudaSuccess ||
-           resolve_per_sm < 1))
-        return LSB_ERR_CUDA;
-      const int rgrid = std::max(1, std::min<int>(num_sms * resolve_per_sm, (int)((m + 255) / 256)));
-      {
-        TableView tv = view();
-        GridBarrier* b = bar;
-        void* args[] = {&tv, &sc, &w, &b, &dev_epoch};
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(rgrid);
-        cfg.blockDim = dim3(256);
-        cfg.dynamicSmemBytes = kSortSmemBytes;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_resolve<Tr>, args));
-      }
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resolve_per_sm, k_resolve<Tr>, 256, 0) !=
+              cudaSuccess)
+        resolve_per_sm = 4;
+      const int rgrid =
+          std::max(1, std::min<int>(num_sms * std::max(1, resolve_per_sm), (int)((m + 255) / 256)));
+      k_resolve<Tr><<<rgrid, 256, 0, s>>>(view(), sc, w, bar, dev_epoch);
       LSB_CK(cudaGetLastError());
       if (overlap)
         if (int e2 = span_mark(wi, 5, s)) return e2;
@@ -1461,11 +1488,22 @@ struct Table {
     return LSB_OK;
   }
 
-  // Ordering of the window's big groups (k_sort; its hot-key steps finish in
-  // k_resolve).
+  // Ordering of the window's big groups (k_sort, a cooperative launch: its
+  // hot-key steps have grid barriers).
   int launch_sort(Window<Tr> w, cudaStream_t s, const uint32_t* dev_epoch) {
-    k_sort<Tr><<<num_sms, LSB_SORT_THREADS, kSortSmemBytes, s>>>(sc, w, dev_epoch);
-    LSB_CK(cudaGetLastError());
+    GridBarrier* b = bar;
+    void* args[] = {&sc, &w, &b, &dev_epoch};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(num_sms);
+    cfg.blockDim = dim3(LSB_SORT_THREADS);
+    cfg.dynamicSmemBytes = kSortSmemBytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LSB_CK(cudaLaunchKernelExC(&cfg, (const void*)k_sort<Tr>, args));
     return LSB_OK;
   }
 
